@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 n-space path tracer: paths/s on the n = 4 measured scene.
+
+Workload (the configuration the metric is quoted on): the boundary of the convex hull of 100,000
+seeded points on the unit 3-sphere (675,456 tetrahedra) above a 4-parallelotope floor
+[-4,4]^3 x [-1.1,-1], a point light at (2,2,2,3), parallel projection onto a 128^3 screen, 16 samples
+per pixel (27 after stratification), recursion depth 5, FP32 with the FP64 re-test.  One step = one
+full frame (56,623,104 camera paths).  The scene arrays (~400 MB) exceed the 126 MB L2, so no L2 flush
+is needed between steps.
+
+--impl ours (default): the sm_100a wavefront through the C ABI.  value: paths/s, device-timed with
+CUDA events on the scene's stream over K steps (max over ranks); e2e: the same through the public API
+with the scene's arrays copied from pinned host memory and the image read back every step.
+--impl reference: the reference painter (oracle/_ref, compiled from the reference's own sources) on
+the host's cores, each step a seeded random pixel sample of the same frame.
+
+Multi-GPU (torchrun): every rank renders the whole frame with its own sample range (weak scaling);
+the per-pixel sums are combined with one NCCL all-reduce after the timed region.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {"n3": "n3", "n4": "n4", "n5": "n5"}
+METRIC = "paths/s per n (n=4 plain tracer)"
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms while the timed region runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            if self.thread:
+                self.thread.join(timeout=2)
+
+    def summary(self) -> dict:
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = max(mx, float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def algorithmic_work(n: int, facet_tests: int, box_steps: int, descent: int) -> tuple[int, int]:
+    """Bytes and flops of the reference algorithm's tree walk for the given counts (per unit:
+    a descent level reads one box, 2n floats; a visited leaf one exit slab, 2n floats; a facet test
+    one index and one simplex record, n^2 + 2n - 1 floats; flops: 2n per level, 6n per slab,
+    2n^2 + 4n per facet test)."""
+    b = descent * 2 * n * 4 + box_steps * 2 * n * 4 + facet_tests * ((n * n + 2 * n - 1) * 4 + 4)
+    f = descent * 2 * n + box_steps * 6 * n + facet_tests * (2 * n * n + 4 * n)
+    return b, f
+
+
+def cpu_baseline(spec: dict, paths_target: int, threads: int) -> dict:
+    """The reference painter on the host cores over a seeded random pixel sample of the frame."""
+    from oracle import checkers
+
+    n = spec["n"]
+    screen = spec["projector"]["screen"]
+    npix = int(np.prod(screen))
+    spp_eff = checkers.Port().effective_spp(n, spec["spp"])
+    count = int(min(npix, max(1000, paths_target // spp_eff)))
+    rng = np.random.default_rng(12345)
+    lin = np.sort(rng.choice(npix, count, replace=False))
+    px = np.empty((count, n - 1), np.int64)
+    rem = lin.copy()
+    for j in range(n - 1):
+        px[:, j] = rem % screen[j]
+        rem //= screen[j]
+    if checkers.Reference.available():
+        ref = checkers.Reference()
+        _, st = ref.paint(spec, dbl=False, seed=1, threads=threads, pixels=px, store=False)
+        return {"value": st["sample_count"] / st["seconds"], "unit": "paths/s", "cores": threads,
+                "kind": "reference", "seconds": st["seconds"],
+                "sample": f"{count} random pixels of the {'x'.join(map(str, screen))} frame x {spp_eff} spp "
+                          f"= {st['sample_count']} paths, paint<{n},float>() with {threads} threads"}
+    port = checkers.Port()
+    _, st = port.paint(spec, dbl=False, threads=threads, pixels=px)
+    return {"value": st["paths"] / st["seconds"], "unit": "paths/s", "cores": threads, "kind": "port",
+            "seconds": st["seconds"],
+            "sample": f"{count} random pixels x {spp_eff} spp with the C restatement, {threads} threads"}
+
+
+def run_reference(args) -> None:
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from math_b200 import scenes
+    from oracle import checkers
+
+    spec = scenes.config(args.config)
+    threads = os.cpu_count() or 1
+    n = spec["n"]
+    if not checkers.Reference.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_painter.so is not built"}))
+        return
+    ref = checkers.Reference()
+    screen = spec["projector"]["screen"]
+    npix = int(np.prod(screen))
+    spp_eff = checkers.Port().effective_spp(n, spec["spp"])
+    count = min(npix, args.cpu_paths // spp_eff)
+    rng = np.random.default_rng(7)
+    total_paths, total_s = 0, 0.0
+    for step in range(args.warmup + args.steps):
+        lin = np.sort(rng.choice(npix, count, replace=False))
+        px = np.stack([(lin // int(np.prod(screen[:j]))) % screen[j] for j in range(n - 1)], axis=1)
+        _, st = ref.paint(spec, dbl=False, seed=step + 1, threads=threads, pixels=px, store=False)
+        if step >= args.warmup:
+            total_paths += st["sample_count"]
+            total_s += st["seconds"]
+    value = total_paths / total_s
+    sample = (f"per step {count} random pixels of the {'x'.join(map(str, screen))} frame x {spp_eff} spp, "
+              f"paint<{n},float>() of the reference with {threads} threads")
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_block(spec, args),
+        "cpu_baseline": {"value": value, "unit": "paths/s", "cores": threads, "kind": "reference", "sample": sample},
+        "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def config_block(spec: dict, args) -> dict:
+    n = spec["n"]
+    return {"workload": f"n={n} plain tracer: {len(spec['facets'])}-facet sphere hull mesh + floor + point light, "
+                        f"parallel projection {'x'.join(map(str, spec['projector']['screen']))}, "
+                        f"{spec['spp']} spp, depth {spec['max_depth']}, FP32 + FP64 re-test",
+            "n": n, "facets": int(len(spec["facets"])), "screen": spec["projector"]["screen"], "spp": spec["spp"],
+            "max_depth": spec["max_depth"], "seed": spec["seed"],
+            "l2": "scene arrays larger than the 126 MB L2; no flush between steps"}
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="n4")
+    ap.add_argument("--cpu-paths", type=int, default=8_000_000, help="paths in the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    if args.impl == "reference":
+        run_reference(args)
+        return
+
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    os.environ.setdefault("NTRACE_NO_BUILD", "1")
+    from math_b200 import scenes
+
+    spec = scenes.config(args.config)
+    n = spec["n"]
+    scene = scenes.build_scene(spec)
+    spp, depth = spec["spp"], spec["max_depth"]
+    stream = torch.cuda.ExternalStream(scene.stream)
+
+    # warm-up (also the per-kernel timing pass: device events around every launch)
+    for _ in range(args.warmup - 1):
+        scene.render(spp, max_depth=depth, seed=spec["seed"] + rank)
+    timed = scene.render(spp, max_depth=depth, seed=spec["seed"] + rank, timing=True)
+    scene.clear()
+
+    # timed region: K frames, device time between two events on the scene's stream
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(local) as clocks:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            stats.append(scene.render(spp, max_depth=depth, seed=spec["seed"] + rank))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    paths = sum(s["paths"] for s in stats)
+    launches = sum(s["launches"] for s in stats)
+    errors = sum(s["error_bits"] for s in stats)
+    ms_all = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    paths_all = torch.tensor([paths], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(ms_all, op=dist.ReduceOp.MAX)
+        dist.all_reduce(paths_all, op=dist.ReduceOp.SUM)
+    ms_max = float(ms_all.item())
+    value = float(paths_all.item()) / (ms_max / 1000.0)
+
+    # combine the ranks' sample ranges into one image (one NCCL all-reduce of the per-pixel sums)
+    combine_ms = None
+    if dist:
+        img, spp_done = scene.image()
+        sums = torch.from_numpy(img.astype(np.float64) * spp_done).cuda()
+        t0 = time.perf_counter()
+        dist.all_reduce(sums)
+        torch.cuda.synchronize()
+        combine_ms = 1000 * (time.perf_counter() - t0)
+
+    # end to end through the public API: upload the scene arrays from pinned host memory, render,
+    # read the image back, every step (wall clock around the calls)
+    scene.clear()
+    e2e_steps = max(1, min(args.steps, 5))
+    h2d = d2h = 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e2e_paths = 0
+    for _ in range(e2e_steps):
+        h2d = scene.upload()
+        st = scene.render(spp, max_depth=depth, seed=spec["seed"] + rank)
+        img, _ = scene.image()
+        e2e_paths += st["paths"]
+        d2h = scene.pixel_count * 3 * 8
+    e2e_s = time.perf_counter() - t0
+    e2e_all = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
+    e2e_value = e2e_paths * world / float(e2e_all.item())
+
+    # roofline of the dominant kernel (extension), from the timed warm-up pass
+    peaks = measured_peaks()
+    ext_bytes, ext_flops = algorithmic_work(n, timed["facet_tests"], timed["box_steps"], timed["descent_levels"])
+    sh_bytes, _ = algorithmic_work(n, timed["shadow_facet_tests"], timed["shadow_box_steps"],
+                                   timed["shadow_descent_levels"])
+    ext_launch_ms = timed["extend_ms"] / max(1, timed["extend_launches"])
+    achieved = (ext_bytes / max(1, timed["extend_launches"])) / (ext_launch_ms / 1000.0) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            traffic = json.loads(tf.read_text()).get(f"{args.config}_extend_bytes_per_launch")
+        except Exception:
+            traffic = None
+
+    result = {
+        "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_block(spec, args),
+        "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "steps": e2e_steps},
+        "gpu_launches": launches,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": "k_extend",
+                     "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_launch": ext_bytes / max(1, timed["extend_launches"]),
+                     "algorithmic_flops_per_launch": ext_flops / max(1, timed["extend_launches"]),
+                     "launch_ms": ext_launch_ms},
+        "kernels_ms_per_frame": {"raygen": timed["raygen_ms"], "extend": timed["extend_ms"], "shade": timed["shade_ms"],
+                                 "shadow": timed["shadow_ms"]},
+        "shadow_algorithmic_gbs": (sh_bytes / (timed["shadow_ms"] / 1000.0) / 1e9) if timed["shadow_ms"] else None,
+        "counters_per_frame": {k: timed[k] for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests",
+                                                     "descent_levels", "shadow_facet_tests", "shadow_box_steps",
+                                                     "shadow_retests", "shadow_descent_levels")},
+        "clocks": clocks.summary(),
+        "device_errors": errors,
+    }
+    if combine_ms is not None:
+        result["combine_ms"] = combine_ms
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        result["cpu_baseline"] = cpu_baseline(spec, args.cpu_paths, os.cpu_count() or 1)
+    if rank == 0:
+        print(json.dumps(result))
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,205 @@
+/*
+ * ntrace: B200 (sm_100a) n-space path tracer, C ABI.
+ *
+ * Drop-in boundary for the CPU painter of templeblock/math (src/painter).  The reference is
+ * in-process C++: a caller assembles a PaintObjects<N,T> (objects, light sources, projector, default
+ * surface; src/painter/objects.h:141-223) and calls
+ *     paint<N,T>(notifier, samples_per_pixel, paint_objects, paintbrush, thread_count, stop, smooth_normal)
+ * (src/painter/painter.h:40-42, src/painter/painter.cpp:599-625).  This header exposes the same scene
+ * vocabulary as plain C: one nt_scene per PaintObjects, one add_* call per visible object or light,
+ * nt_render for paint().  The C++ header math_b200/paint.hpp rebuilds the reference's template
+ * interface on top of it.
+ *
+ * Conventions: n is the space dimension (3..6); the screen has n-1 dimensions; every vector is n
+ * floats, every edge list is row-major; pixels are linear with x0 fastest (GlobalIndex,
+ * src/com/global_index.h:45-147).  Host arrays are copied by the call that receives them.  Every
+ * function returns an NT_* status; nt_last_error_message() describes the last failure on the
+ * calling thread.  Nothing throws across the ABI (the reference's paint() is noexcept and reports
+ * through its notifier, painter.cpp:598-625).  One scene must not be used by two threads at once;
+ * separate scenes may render concurrently (each owns a CUDA stream).
+ */
+#ifndef NTRACE_H
+#define NTRACE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define NT_OK 0
+#define NT_EINVAL 1       /* invalid argument or scene */
+#define NT_EDEGENERATE 2  /* degenerate geometry (e.g. a simplex whose normal is not finite) */
+#define NT_ECUDA 3        /* CUDA runtime error */
+#define NT_ETIMEOUT 4     /* a bounded device loop ran out (walk or sampler bound) */
+#define NT_ESTOPPED 5     /* stopped through the stop flag */
+#define NT_ENOMEM 6       /* device allocation failed */
+#define NT_ESTATE 7       /* call out of order (e.g. render before build) */
+
+typedef struct nt_scene nt_scene;
+
+/* SurfaceProperties subset used by the painter (src/painter/objects.h:26-133). */
+typedef struct nt_surface
+{
+        float color[3];        /* linear RGB */
+        float diffuse;         /* diffuse coefficient; 0 disables direct and indirect lighting */
+        int light_source;      /* the surface emits light_color */
+        float light_color[3];
+} nt_surface;
+
+/* Projector kinds (src/painter/projectors/projector.h). */
+#define NT_PROJECTOR_PARALLEL 0     /* param: units per pixel */
+#define NT_PROJECTOR_PERSPECTIVE 1  /* param: width view angle, degrees */
+#define NT_PROJECTOR_SPHERICAL 2    /* param: width view angle, degrees */
+
+typedef struct nt_build_opts
+{
+        int threads;   /* host threads for the tree build; <= 0: all hardware threads */
+        int host_only; /* 1: facet setup and tree build only, no device upload (inspection on hosts
+                          without a GPU; render and trace calls then fail with NT_ESTATE) */
+} nt_build_opts;
+
+typedef struct nt_render_opts
+{
+        int samples_per_pixel;  /* rounded up to k^(n-1) as StratifiedJitteredSampler does (sampler.h:31-52) */
+        int max_depth;          /* MAX_RECURSION_LEVEL (painter.cpp:42); the reference value is 100 */
+        uint64_t seed;          /* Philox key; path id = (sample index) * pixel_count + pixel */
+        int retest;             /* 1: re-test uncertain FP32 facet tests in FP64 (default); 0: FP32 only */
+        int smooth_normal;      /* paint()'s smooth_normal; meshes without vertex normals ignore it */
+        int64_t pool_paths;     /* wavefront path pool size; <= 0: automatic */
+        int timing;             /* 1: per-kernel CUDA-event times in nt_stats */
+        const volatile int* stop; /* optional host stop flag, polled between wavefront iterations */
+} nt_render_opts;
+
+typedef struct nt_stats
+{
+        int64_t paths;            /* camera samples traced (BarPaintbrush sample_count) */
+        int64_t rays;             /* extension rays traced */
+        int64_t shadow_rays;      /* shadow rays traced */
+        int64_t facet_tests;      /* ray-simplex tests */
+        int64_t box_steps;        /* tree leaves visited */
+        int64_t retests;          /* FP64 re-tests */
+        int64_t descent_levels;   /* tree nodes visited by point location */
+        int64_t error_bits;       /* device error flags (bounded loops that ran out) */
+        int spp_effective;        /* samples per pixel actually traced */
+        double seconds;           /* host wall time of the call */
+        double raygen_ms;         /* device times per kernel kind (timing = 1) */
+        double extend_ms;
+        double shade_ms;
+        double shadow_ms;
+        int64_t launches;         /* kernel launches issued by the call */
+        int64_t extend_launches;
+        int64_t shadow_launches;
+        /* the shadow kernel's walk counters (facet_tests .. descent_levels above count extension rays) */
+        int64_t shadow_facet_tests;
+        int64_t shadow_box_steps;
+        int64_t shadow_retests;
+        int64_t shadow_descent_levels;
+} nt_stats;
+
+typedef struct nt_mesh_info
+{
+        int64_t facet_count;
+        int64_t node_count;       /* tree boxes */
+        int64_t leaf_count;
+        int64_t index_count;      /* facet references held by leaves */
+        int max_depth;            /* tree_max_depth (src/painter/shapes/mesh.cpp:35-58) */
+        double distance_from_facet;
+        int64_t degenerate_facets; /* facets decided in FP64 only (ill-conditioned barycentric solve) */
+        double build_seconds;
+        int64_t device_bytes;
+} nt_mesh_info;
+
+/* ---- scene assembly (PaintObjects) ---- */
+
+/* Replaces constructing a PaintObjects<N,T> (objects.h:211-223); n = 3..6. */
+int nt_scene_create(int n, nt_scene** out);
+int nt_scene_destroy(nt_scene* scene);
+
+/* Mesh of (n-1)-simplices: Mesh<N,T>(obj, ...) + VisibleSharedMesh (mesh.cpp:61-135,
+ * visible_shapes.h:119-168).  vertices: vertex_count x n; facets: facet_count x n vertex indices. */
+int nt_scene_add_mesh(nt_scene* scene, const float* vertices, int64_t vertex_count, const int32_t* facets,
+                      int64_t facet_count, const nt_surface* surface);
+
+/* n-parallelotope: VisibleParallelotope(org, e0..e(n-1)) (visible_shapes.h:75-117).  edges: n x n. */
+int nt_scene_add_parallelotope(nt_scene* scene, const float* org, const float* edges, const nt_surface* surface);
+
+/* (n-1)-parallelotope in a hyperplane: VisibleHyperplaneParallelotope (visible_shapes.h:31-73).
+ * edges: (n-1) x n. */
+int nt_scene_add_hyperplane_parallelotope(nt_scene* scene, const float* org, const float* edges,
+                                          const nt_surface* surface);
+
+/* VisiblePointLight(location, color, unit_intensity_distance) (visible_lights.h:24-39,
+ * light_source.h:26-57). */
+int nt_scene_add_point_light(nt_scene* scene, const float* location, const float* rgb, float unit_intensity_distance);
+
+/* VisibleConstantLight(location, color) (visible_lights.h:41-55, light_source.h:59-78). */
+int nt_scene_add_constant_light(nt_scene* scene, const float* location, const float* rgb);
+
+/* Visible{Parallel,Perspective,Spherical}Projector (visible_projectors.h:24-94).  screen_axes:
+ * (n-1) x n; screen_size: n-1 ints. */
+int nt_scene_set_projector(nt_scene* scene, int kind, const float* camera_org, const float* camera_dir,
+                           const float* screen_axes, float param, const int32_t* screen_size);
+
+/* PaintObjects::default_surface_properties (objects.h:222): what a ray that hits nothing returns. */
+int nt_scene_set_background(nt_scene* scene, const nt_surface* surface);
+
+/* Facet setup, 2^n-tree build and upload to the device (the work of Mesh's constructor). */
+int nt_scene_build(nt_scene* scene, const nt_build_opts* opts);
+
+int nt_scene_mesh_info(nt_scene* scene, int mesh_index, nt_mesh_info* info);
+
+/* ---- painting (paint<N,T>) ---- */
+
+/* One pass: samples_per_pixel (stratified, effective count k^(n-1)) more samples for every pixel
+ * of the screen, added to the scene's accumulator; successive calls continue the sample sequence. */
+int nt_render(nt_scene* scene, const nt_render_opts* opts, nt_stats* stats);
+
+int nt_accum_clear(nt_scene* scene);
+
+/* Mean colour per pixel (pixel_count x 3 floats, x0 fastest) and the samples behind it. */
+int nt_accum_read(nt_scene* scene, float* rgb_mean, int64_t* samples_per_pixel);
+
+int64_t nt_scene_pixel_count(nt_scene* scene);
+
+/* Copies the scene's device arrays again from the pinned host copy the build kept (a scene whose
+ * data arrive from the host for every frame); *bytes: host-to-device bytes moved.  No counterpart in
+ * the reference, whose scene lives in host memory. */
+int nt_scene_upload(nt_scene* scene, int64_t* bytes);
+
+/* The scene's CUDA stream (cudaStream_t), on which nt_render and nt_trace_closest launch. */
+void* nt_scene_stream(nt_scene* scene);
+
+/* ---- fixed-ray-set closest hit (parity checks) ---- */
+
+/* Closest facet of mesh mesh_index for each ray, as Mesh::intersect_approximate followed by
+ * Mesh::intersect_precise (mesh.cpp:137-166; the query of shapes/test/test_mesh.cpp:139-152).
+ * org, dir: ray_count x n host floats (dir need not be unit); facet: -1 for a miss; t: distance
+ * from org along the unit direction.  retest = 1 settles uncertain FP32 decisions in FP64. */
+int nt_trace_closest(nt_scene* scene, int mesh_index, const float* org, const float* dir, int64_t ray_count,
+                     int retest, int32_t* facet, float* t, nt_stats* stats);
+
+/* Same with device pointers on the caller's stream (cudaStream_t; NULL = the scene's stream). */
+int nt_trace_closest_device(nt_scene* scene, int mesh_index, const float* d_org, const float* d_dir,
+                            int64_t ray_count, int retest, int32_t* d_facet, float* d_t, void* stream);
+
+/* Tree export (host copies) for checks: node_count int2 nodes ({first_child, -1} or {offset, count}),
+ * index_count leaf facet indices, per-level box sizes ((max_depth + 1) x n) and root origin (n). */
+int nt_scene_tree_export(nt_scene* scene, int mesh_index, int32_t* nodes, int32_t* indices, float* level_sizes,
+                         float* root_org);
+
+/* ---- misc ---- */
+
+const char* nt_last_error_message(void);
+
+/* Samples per pixel that samples_per_pixel becomes in n dimensions. */
+int nt_effective_spp(int n, int samples_per_pixel);
+
+/* cosine_sphere_coefficient(n) (src/painter/coefficient/cosine_sphere.h:97-162). */
+double nt_cosine_sphere_coefficient(int n);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

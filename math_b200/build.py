@@ -1,0 +1,88 @@
+"""Builds the in-tree shared library math_b200/libntrace.so (C ABI: include/ntrace.h).
+
+The CUDA kernels are compiled for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``) with
+``-fmad=false`` so that every fused multiply-add is an explicit one, and the host code with
+``-ffp-contract=off`` so that its float arithmetic follows the reference's operation order (the tree
+built here is the tree the reference's Mesh<N,float> builds).  The CUDA runtime is linked statically,
+so the library only needs the driver at run time.
+"""
+
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent
+CSRC = HERE / "csrc"
+INCLUDE = ROOT / "include"
+LIB = HERE / "libntrace.so"
+BUILD_DIR = ROOT / "_build" / "ntrace"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    cuda_home = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    nvcc = Path(cuda_home) / "bin" / "nvcc"
+    if nvcc.exists():
+        return str(nvcc)
+    found = shutil.which("nvcc")
+    if not found:
+        raise RuntimeError("nvcc not found; the CUDA toolkit is required to build ntrace")
+    return found
+
+
+def _run(cmd: list[str]) -> None:
+    proc = subprocess.run(cmd, capture_output=True, text=True)
+    if proc.returncode != 0:
+        sys.stderr.write(proc.stdout + proc.stderr)
+        raise RuntimeError("command failed: " + " ".join(cmd))
+
+
+def _stale(target: Path, sources: list[Path]) -> bool:
+    if not target.exists():
+        return True
+    t = target.stat().st_mtime
+    return any(s.stat().st_mtime > t for s in sources)
+
+
+def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) -> Path:
+    """Compiles libntrace.so if any source is newer than it; returns its path."""
+    nvcc = _nvcc()
+    headers = sorted(CSRC.glob("*.h")) + sorted(CSRC.glob("*.hpp")) + sorted(CSRC.glob("*.cuh")) + [INCLUDE / "ntrace.h"]
+    cu = CSRC / "kernels.cu"
+    cpp = CSRC / "scene.cpp"
+    BUILD_DIR.mkdir(parents=True, exist_ok=True)
+    cu_obj = BUILD_DIR / "kernels.o"
+    cpp_obj = BUILD_DIR / "scene.o"
+    common = ["-std=c++17", "-I", str(INCLUDE), "-I", str(CSRC)]
+    if force or _stale(cu_obj, [cu] + headers):
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", *common,
+               "-c", str(cu), "-o", str(cu_obj)]
+        if ptxas_info:
+            cmd.insert(1, "-Xptxas=-v")
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    if force or _stale(cpp_obj, [cpp] + headers):
+        cmd = [nvcc, "-x", "c++", "-Wno-deprecated-gpu-targets", "-O2", "-Xcompiler", "-fPIC,-ffp-contract=off,-pthread", *common, "-c", str(cpp),
+               "-o", str(cpp_obj)]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    if force or _stale(LIB, [cu_obj, cpp_obj]):
+        cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj), "-Xlinker",
+               "--no-undefined", "-lpthread"]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv, verbose=True, ptxas_info="--ptxas" in sys.argv)
+    print(LIB)

@@ -1,0 +1,673 @@
+// sm_100a kernels of the n-space path tracer: the fixed-ray-set closest-hit query and the
+// wavefront (ray generation, extension, shading, shadow rays, accumulation) with path and shadow
+// queues compacted by warp ballot plus block prefix sums.
+#include "device.cuh"
+#include "kernels.h"
+
+#include <cuda_runtime.h>
+
+namespace ntrace
+{
+namespace
+{
+constexpr int BLOCK = 256;
+
+__device__ __forceinline__ unsigned lanemask_lt()
+{
+        unsigned m;
+        asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+        return m;
+}
+
+// Block-wide stream compaction slot: every thread of the block must call it (flag may be false).
+// Warp ballot + popc give the in-warp prefix, a shared-memory scan over warps gives the block
+// offset, and one atomic per block reserves the block's range in the output queue.
+__device__ __forceinline__ long long compact_slot(bool flag, unsigned long long* counter, int* s_warp, long long* s_base)
+{
+        const int lane = threadIdx.x & 31;
+        const int warp = threadIdx.x >> 5;
+        unsigned ballot = __ballot_sync(0xffffffffu, flag);
+        if (lane == 0)
+        {
+                s_warp[warp] = __popc(ballot);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0)
+        {
+                int total = 0;
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                {
+                        int c = s_warp[w];
+                        s_warp[w] = total;
+                        total += c;
+                }
+                *s_base = total ? (long long)atomicAdd(counter, (unsigned long long)total) : 0;
+        }
+        __syncthreads();
+        long long slot = *s_base + s_warp[warp] + __popc(ballot & lanemask_lt());
+        __syncthreads();
+        return flag ? slot : -1;
+}
+
+template <bool SHADOW_KERNEL>
+__device__ __forceinline__ void flush_stats(unsigned long long* counters, const WalkStats& ws, long long rays,
+                                            long long shadow_rays)
+{
+        if (!counters)
+        {
+                return;
+        }
+        warp_add(counters + (SHADOW_KERNEL ? C_SH_FACET_TESTS : C_FACET_TESTS), ws.facet_tests);
+        warp_add(counters + (SHADOW_KERNEL ? C_SH_BOX_STEPS : C_BOX_STEPS), ws.box_steps);
+        warp_add(counters + (SHADOW_KERNEL ? C_SH_RETESTS : C_RETESTS), ws.retests);
+        warp_add(counters + (SHADOW_KERNEL ? C_SH_DESCENT : C_DESCENT), ws.descent);
+        warp_add(counters + C_RAYS, rays);
+        warp_add(counters + C_SHADOW_RAYS, shadow_rays);
+        if (ws.error)
+        {
+                atomicOr((unsigned long long*)(counters + C_ERROR), (unsigned long long)ws.error);
+        }
+}
+
+// ------------------------------------------------------------------------------------------------
+// Fixed ray set: closest facet per ray through Mesh::intersect_approximate + intersect_precise
+// (the query of src/painter/shapes/test/test_mesh.cpp:139-152).
+
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_trace_closest(__grid_constant__ const MeshDev<N> M, const float* __restrict__ org,
+                                                         const float* __restrict__ dir, long long nrays, int retest,
+                                                         int* __restrict__ facet_out, float* __restrict__ t_out,
+                                                         unsigned long long* counters)
+{
+        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        WalkStats ws{0, 0, 0, 0, 0};
+        if (i < nrays)
+        {
+                float o[N], d[N];
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        o[k] = org[i * N + k];
+                        d[k] = dir[i * N + k];
+                }
+                Ray<N> r;
+                ray_set<N>(r, o, d);
+                Ray64Source<N> src{org, dir, i};
+                float first, second;
+                int f = -1;
+                float t = 0;
+                if (root_slabs<N>(M, r.org, r.dir, &first, &second))
+                {
+                        float a = (first > 0) ? first : second;
+                        if (!mesh_closest<N>(M, r, a, src, retest, FLT_MAX, &t, &f, &ws))
+                        {
+                                f = -1;
+                                t = 0;
+                        }
+                }
+                facet_out[i] = f;
+                t_out[i] = t;
+        }
+        flush_stats<false>(counters, ws, i < nrays ? 1 : 0, 0);
+}
+
+// ------------------------------------------------------------------------------------------------
+// Wavefront
+
+template <int N>
+struct PathView
+{
+        float* f;        // (2N + 4) x Q: org[N], dir[N], beta[3], color_level
+        uint32_t* pix;   // Q
+        uint32_t* smp;   // Q: sample index of the pixel (pass offset included)
+        int* level;      // Q: bounce level; level > 0 means the ray is a diffuse bounce
+        long long Q;
+
+        __device__ __forceinline__ float& at(int field, long long i) const
+        {
+                return f[field * Q + i];
+        }
+};
+
+template <int N>
+struct HitView
+{
+        float* t;
+        int* obj;
+        int* facet;
+};
+
+template <int N>
+struct ShadowView
+{
+        float* f;        // (2N + 4) x Q: org[N], dir[N], tmax, contrib[3]
+        uint32_t* pix;
+        long long Q;
+
+        __device__ __forceinline__ float& at(int field, long long i) const
+        {
+                return f[field * Q + i];
+        }
+};
+
+// paint_pixels: stratified jittered sample -> projector ray (painter.cpp:410-448,
+// sampler.h:26-64, engine.h:86-156)
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, long long first_slot,
+                                                  long long count)
+{
+        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i >= count)
+        {
+                return;
+        }
+        long long g = P.path_begin + i;
+        long long pixel = g / P.spp_eff;
+        int s = (int)(g - pixel * P.spp_eff);
+        long long sample = P.sample_offset + s;
+        unsigned long long path = (unsigned long long)sample * (unsigned long long)P.npix + (unsigned long long)pixel;
+
+        int px[N - 1];
+        long long rem = pixel;
+#pragma unroll
+        for (int j = 0; j < N - 1; ++j)
+        {
+                px[j] = (int)(rem % S.proj.screen[j]);
+                rem /= S.proj.screen[j];
+        }
+        float u[8];
+        float4 a = rng4(P.key0, P.key1, path, 0, 0);
+        u[0] = a.x;
+        u[1] = a.y;
+        u[2] = a.z;
+        u[3] = a.w;
+        if constexpr (N - 1 > 4)
+        {
+                float4 b = rng4(P.key0, P.key1, path, 0, 1);
+                u[4] = b.x;
+        }
+        float point[N - 1];
+        int r = s;
+#pragma unroll
+        for (int j = 0; j < N - 1; ++j)
+        {
+                int digit = r % P.k1d;
+                r /= P.k1d;
+                float offset = __fdiv_rn((float)digit, (float)P.k1d);
+                float sample_j = offset + u[j] * P.recip_k;
+                point[j] = (float)px[j] + sample_j;
+        }
+        Ray<N> ray;
+        projector_ray<N>(S.proj, point, ray);
+        long long slot = first_slot + i;
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+        {
+                A.at(k, slot) = ray.org[k];
+                A.at(N + k, slot) = ray.dir[k];
+        }
+        A.at(2 * N + 0, slot) = 1.0f;
+        A.at(2 * N + 1, slot) = 1.0f;
+        A.at(2 * N + 2, slot) = 1.0f;
+        A.at(2 * N + 3, slot) = 1.0f;
+        A.pix[slot] = (uint32_t)pixel;
+        A.smp[slot] = (uint32_t)sample;
+        A.level[slot] = 0;
+}
+
+// extension: closest object per path (ray_intersection over objects, ray_intersection.h:26-105)
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, long long count,
+                                                  unsigned long long* counters)
+{
+        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        WalkStats ws{0, 0, 0, 0, 0};
+        if (i < count)
+        {
+                Ray<N> r;
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        r.org[k] = A.at(k, i);
+                        r.dir[k] = A.at(N + k, i);
+                }
+                float t;
+                int obj, facet;
+                if (scene_closest<N>(S, r, &t, &obj, &facet, &ws))
+                {
+                        H.t[i] = t;
+                        H.obj[i] = obj;
+                        H.facet[i] = facet;
+                }
+                else
+                {
+                        H.obj[i] = -1;
+                }
+        }
+        flush_stats<false>(counters, ws, i < count ? 1 : 0, 0);
+}
+
+__device__ __forceinline__ void accumulate(double* accum, uint32_t pixel, float r, float g, float b)
+{
+        double* p = accum + (size_t)pixel * 3;
+        atomicAdd(p + 0, (double)r);
+        atomicAdd(p + 1, (double)g);
+        atomicAdd(p + 2, (double)b);
+}
+
+// shading: trace_path / direct_diffuse_lighting / diffuse_lighting (painter.cpp:197-397).  A miss
+// or an emitting hit adds its colour to the pixel; a diffuse hit emits one shadow ray per light into
+// the shadow queue and, below the depth cap, writes its continuation into the next path queue.
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, HitView<N> H,
+                                                 PathView<N> B, ShadowView<N> SQ, double* accum, long long count,
+                                                 unsigned long long* counters)
+{
+        __shared__ int s_warp[BLOCK / 32];
+        __shared__ long long s_base;
+        const long long tiles = (count + blockDim.x - 1) / blockDim.x;
+        for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
+        {
+                long long i = tile * blockDim.x + threadIdx.x;
+                bool lit = false;  // diffuse hit whose direct lighting is evaluated
+                float beta[3] = {0, 0, 0};
+                float sc[3] = {0, 0, 0};
+                float ncl = 0;
+                float p[N], gn[N], sn[N];
+                bool mesh = false;
+                uint32_t pixel = 0, sample = 0;
+                int level = 0;
+                int err = 0;
+                if (i < count)
+                {
+                        pixel = A.pix[i];
+                        sample = A.smp[i];
+                        level = A.level[i];
+                        beta[0] = A.at(2 * N + 0, i);
+                        beta[1] = A.at(2 * N + 1, i);
+                        beta[2] = A.at(2 * N + 2, i);
+                        float color_level = A.at(2 * N + 3, i);
+                        Ray<N> ray;
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                ray.org[k] = A.at(k, i);
+                                ray.dir[k] = A.at(N + k, i);
+                        }
+                        int obj = H.obj[i];
+                        bool diffuse_reflection = level > 0;
+                        if (obj < 0)
+                        {
+                                const float* c = (S.bg_light && diffuse_reflection) ? S.bg_light_color : S.bg_color;
+                                accumulate(accum, pixel, beta[0] * c[0], beta[1] * c[1], beta[2] * c[2]);
+                        }
+                        else
+                        {
+                                ray_point<N>(ray, H.t[i], p);
+                                const ObjDev& ob = S.obj[obj];
+                                if (ob.kind == OBJ_MESH)
+                                {
+                                        const float4* rec = S.mesh[ob.index].rec32 + (size_t)H.facet[i] * Rec32<N>::F4;
+                                        float f4[(N + 3) / 4 * 4];
+#pragma unroll
+                                        for (int q = 0; q < (N + 3) / 4; ++q)
+                                        {
+                                                float4 v = __ldg(rec + q);
+                                                f4[4 * q + 0] = v.x;
+                                                f4[4 * q + 1] = v.y;
+                                                f4[4 * q + 2] = v.z;
+                                                f4[4 * q + 3] = v.w;
+                                        }
+#pragma unroll
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                gn[k] = f4[k];
+                                        }
+                                }
+                                else if (ob.kind == OBJ_PLT)
+                                {
+                                        plt_normal<N>(S.plt[ob.index], p, gn);
+                                }
+                                else
+                                {
+#pragma unroll
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                gn[k] = S.hplt[ob.index].normal[k];
+                                        }
+                                }
+                                vnormalize<N>(gn);
+                                mesh = ob.kind == OBJ_MESH;
+                                float dd = vdot<N>(ray.dir, gn);
+                                if (!(fabsf(dd) <= 0))
+                                {
+                                        if (ob.light_source)
+                                        {
+                                                const float* c = diffuse_reflection ? ob.light_color : ob.color;
+                                                accumulate(accum, pixel, beta[0] * c[0], beta[1] * c[1], beta[2] * c[2]);
+                                        }
+                                        else
+                                        {
+                                                if (dd > 0)
+                                                {
+#pragma unroll
+                                                        for (int k = 0; k < N; ++k)
+                                                        {
+                                                                gn[k] = -gn[k];
+                                                        }
+                                                }
+#pragma unroll
+                                                for (int k = 0; k < N; ++k)
+                                                {
+                                                        sn[k] = gn[k];
+                                                }
+                                                if (ob.diffuse > 0)
+                                                {
+                                                        sc[0] = ob.diffuse * ob.color[0];
+                                                        sc[1] = ob.diffuse * ob.color[1];
+                                                        sc[2] = ob.diffuse * ob.color[2];
+                                                        ncl = color_level * cmax3(sc);
+                                                        lit = ncl >= 1e-4f;
+                                                }
+                                        }
+                                }
+                        }
+                }
+
+                // direct lighting: one shadow ray per light (block-uniform loop, compacted per light)
+                for (int l = 0; l < S.nlights; ++l)
+                {
+                        bool shadow = false;
+                        float sh_org[N], sh_dir[N], sh_tmax = 0, sh_c[3] = {0, 0, 0};
+                        if (lit)
+                        {
+                                float lc[3], vec[N];
+                                light_properties<N>(S.lights[l], p, lc, vec);
+                                if (!(cmax3(lc) < 1e-4f))
+                                {
+                                        Ray<N> lr;
+                                        ray_set<N>(lr, p, vec);
+                                        float dln = vdot<N>(lr.dir, sn);
+                                        if (dln > 0)
+                                        {
+                                                ray_move<N>(lr, S.ray_offset);
+                                                float w = S.diffuse_coef * dln;
+                                                shadow = true;
+#pragma unroll
+                                                for (int k = 0; k < N; ++k)
+                                                {
+                                                        sh_org[k] = lr.org[k];
+                                                        sh_dir[k] = lr.dir[k];
+                                                }
+                                                sh_tmax = __fsqrt_rn(vdot<N>(vec, vec));
+                                                sh_c[0] = beta[0] * sc[0] * (lc[0] * w);
+                                                sh_c[1] = beta[1] * sc[1] * (lc[1] * w);
+                                                sh_c[2] = beta[2] * sc[2] * (lc[2] * w);
+                                        }
+                                }
+                        }
+                        long long qo = compact_slot(shadow, counters + C_SHADOW, s_warp, &s_base);
+                        if (shadow)
+                        {
+#pragma unroll
+                                for (int k = 0; k < N; ++k)
+                                {
+                                        SQ.at(k, qo) = sh_org[k];
+                                        SQ.at(N + k, qo) = sh_dir[k];
+                                }
+                                SQ.at(2 * N + 0, qo) = sh_tmax;
+                                SQ.at(2 * N + 1, qo) = sh_c[0];
+                                SQ.at(2 * N + 2, qo) = sh_c[1];
+                                SQ.at(2 * N + 3, qo) = sh_c[2];
+                                SQ.pix[qo] = pixel;
+                        }
+                }
+
+                // diffuse continuation (diffuse_lighting, painter.cpp:298-323)
+                bool survive = false;
+                float nr_org[N], nr_dir[N];
+                if (lit && level < S.max_depth)
+                {
+                        unsigned long long path = (unsigned long long)sample * (unsigned long long)P.npix + pixel;
+                        float d[N];
+                        if (cosine_hemisphere<N>(P.key0, P.key1, path, (uint32_t)(1 + level), sn, d))
+                        {
+                                Ray<N> dr;
+                                ray_set<N>(dr, p, d);
+                                if (!(mesh && vdot<N>(dr.dir, gn) <= 0))
+                                {
+                                        ray_move<N>(dr, S.ray_offset);
+                                        survive = true;
+#pragma unroll
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                nr_org[k] = dr.org[k];
+                                                nr_dir[k] = dr.dir[k];
+                                        }
+                                }
+                        }
+                        else
+                        {
+                                err |= ERR_SAMPLING_LIMIT;
+                        }
+                }
+                long long so = compact_slot(survive, counters + C_ACTIVE_OUT, s_warp, &s_base);
+                if (survive)
+                {
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                B.at(k, so) = nr_org[k];
+                                B.at(N + k, so) = nr_dir[k];
+                        }
+                        B.at(2 * N + 0, so) = beta[0] * sc[0];
+                        B.at(2 * N + 1, so) = beta[1] * sc[1];
+                        B.at(2 * N + 2, so) = beta[2] * sc[2];
+                        B.at(2 * N + 3, so) = ncl;
+                        B.pix[so] = pixel;
+                        B.smp[so] = sample;
+                        B.level[so] = level + 1;
+                }
+                if (err)
+                {
+                        atomicOr((unsigned long long*)(counters + C_ERROR), (unsigned long long)err);
+                }
+        }
+}
+
+// shadow rays: light_source_is_visible (painter.cpp:172-186); visible -> add the light's share
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, long long count,
+                                                  unsigned long long* counters)
+{
+        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        WalkStats ws{0, 0, 0, 0, 0};
+        if (i < count)
+        {
+                Ray<N> r;
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        r.org[k] = SQ.at(k, i);
+                        r.dir[k] = SQ.at(N + k, i);
+                }
+                float tmax = SQ.at(2 * N, i);
+                if (scene_visible<N>(S, r, tmax, &ws))
+                {
+                        accumulate(accum, SQ.pix[i], SQ.at(2 * N + 1, i), SQ.at(2 * N + 2, i), SQ.at(2 * N + 3, i));
+                }
+        }
+        flush_stats<true>(counters, ws, 0, i < count ? 1 : 0);
+}
+
+template <int N>
+long long grid_for(long long count)
+{
+        return (count + BLOCK - 1) / BLOCK;
+}
+}
+
+// ------------------------------------------------------------------------------------------------
+// Host-side launchers
+
+template <int N>
+size_t Wavefront<N>::bytes_for(long long Q, int lights)
+{
+        size_t per_path = sizeof(float) * (2 * N + 4) * 2  // path state A and B
+                          + sizeof(uint32_t) * 2 * 2 + sizeof(int) * 2
+                          + sizeof(float) + sizeof(int) * 2  // hit record
+                          + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights;  // shadow queue
+        return per_path * (size_t)Q + 16 * 256;
+}
+
+template <int N>
+void Wavefront<N>::carve(char* base, long long Q, int lights)
+{
+        this->Q = Q;
+        this->lights = lights;
+        auto take = [&](size_t bytes) {
+                char* p = base;
+                base += (bytes + 255) / 256 * 256;
+                return p;
+        };
+        fA = (float*)take(sizeof(float) * (2 * N + 4) * Q);
+        fB = (float*)take(sizeof(float) * (2 * N + 4) * Q);
+        pixA = (uint32_t*)take(sizeof(uint32_t) * Q);
+        pixB = (uint32_t*)take(sizeof(uint32_t) * Q);
+        smpA = (uint32_t*)take(sizeof(uint32_t) * Q);
+        smpB = (uint32_t*)take(sizeof(uint32_t) * Q);
+        lvlA = (int*)take(sizeof(int) * Q);
+        lvlB = (int*)take(sizeof(int) * Q);
+        hit_t = (float*)take(sizeof(float) * Q);
+        hit_obj = (int*)take(sizeof(int) * Q);
+        hit_facet = (int*)take(sizeof(int) * Q);
+        sq_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
+        sq_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
+}
+
+template <int N>
+cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
+                              unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
+                              const volatile int* stop)
+{
+        long long active = 0;
+        long long next = 0;
+        bool flip = false;
+        cudaEvent_t ev[8];
+        const bool timing = times != nullptr;
+        if (timing)
+        {
+                for (auto& e : ev)
+                {
+                        cudaEventCreate(&e);
+                }
+        }
+        const long long path_base = P.path_begin;
+        for (int iter = 0; active > 0 || next < total_paths; ++iter)
+        {
+                if (stop && *stop)
+                {
+                        break;
+                }
+                float* fa = flip ? fB : fA;
+                float* fb = flip ? fA : fB;
+                PathView<N> A{fa, flip ? pixB : pixA, flip ? smpB : smpA, flip ? lvlB : lvlA, Q};
+                PathView<N> B{fb, flip ? pixA : pixB, flip ? smpA : smpB, flip ? lvlA : lvlB, Q};
+                HitView<N> H{hit_t, hit_obj, hit_facet};
+                ShadowView<N> SQ{sq_f, sq_pix, Q * lights};
+
+                long long fresh = std::min(Q - active, total_paths - next);
+                if (timing)
+                {
+                        cudaEventRecord(ev[0], st);
+                }
+                if (fresh > 0)
+                {
+                        PassDev pp = P;
+                        pp.path_begin = path_base + next;
+                        k_raygen<N><<<(unsigned)grid_for<N>(fresh), BLOCK, 0, st>>>(S, pp, A, active, fresh);
+                        next += fresh;
+                        active += fresh;
+                }
+                if (timing)
+                {
+                        cudaEventRecord(ev[1], st);
+                }
+                k_extend<N><<<(unsigned)grid_for<N>(active), BLOCK, 0, st>>>(S, A, H, active, counters);
+                if (timing)
+                {
+                        cudaEventRecord(ev[2], st);
+                }
+                cudaMemsetAsync(counters + C_ACTIVE_OUT, 0, 2 * sizeof(unsigned long long), st);
+                long long shade_blocks = std::min<long long>(grid_for<N>(active), 148LL * 16);
+                k_shade<N><<<(unsigned)shade_blocks, BLOCK, 0, st>>>(S, P, A, H, B, SQ, accum, active, counters);
+                if (timing)
+                {
+                        cudaEventRecord(ev[3], st);
+                }
+                cudaMemcpyAsync(host_counters, counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+                cudaError_t e = cudaStreamSynchronize(st);
+                if (e != cudaSuccess)
+                {
+                        return e;
+                }
+                long long survivors = (long long)host_counters[C_ACTIVE_OUT];
+                long long shadows = (long long)host_counters[C_SHADOW];
+                if (shadows > 0)
+                {
+                        k_shadow<N><<<(unsigned)grid_for<N>(shadows), BLOCK, 0, st>>>(S, SQ, accum, shadows, counters);
+                }
+                if (timing)
+                {
+                        cudaEventRecord(ev[4], st);
+                        cudaEventSynchronize(ev[4]);
+                        float ms;
+                        cudaEventElapsedTime(&ms, ev[0], ev[1]);
+                        times->raygen_ms += ms;
+                        cudaEventElapsedTime(&ms, ev[1], ev[2]);
+                        times->extend_ms += ms;
+                        cudaEventElapsedTime(&ms, ev[2], ev[3]);
+                        times->shade_ms += ms;
+                        cudaEventElapsedTime(&ms, ev[3], ev[4]);
+                        times->shadow_ms += ms;
+                        times->extend_launches += 1;
+                        times->shadow_launches += shadows > 0 ? 1 : 0;
+                        times->launches += (fresh > 0 ? 1 : 0) + 2 + (shadows > 0 ? 1 : 0);
+                        times->extend_rays += active;
+                        times->shadow_rays += shadows;
+                }
+                active = survivors;
+                flip = !flip;
+        }
+        if (timing)
+        {
+                for (auto& e : ev)
+                {
+                        cudaEventDestroy(e);
+                }
+        }
+        return cudaGetLastError();
+}
+
+template <int N>
+cudaError_t launch_trace_closest(const MeshDev<N>& M, const float* org, const float* dir, long long nrays, int retest,
+                                 int* facet, float* t, unsigned long long* counters, cudaStream_t st)
+{
+        if (nrays <= 0)
+        {
+                return cudaSuccess;
+        }
+        k_trace_closest<N><<<(unsigned)grid_for<N>(nrays), BLOCK, 0, st>>>(M, org, dir, nrays, retest, facet, t, counters);
+        return cudaGetLastError();
+}
+
+#define NT_INSTANTIATE(N)                                                                                         \
+        template struct Wavefront<N>;                                                                             \
+        template cudaError_t launch_trace_closest<N>(const MeshDev<N>&, const float*, const float*, long long, int, \
+                                                     int*, float*, unsigned long long*, cudaStream_t);
+NT_INSTANTIATE(3)
+NT_INSTANTIATE(4)
+NT_INSTANTIATE(5)
+NT_INSTANTIATE(6)
+#undef NT_INSTANTIATE
+}

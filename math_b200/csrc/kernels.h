@@ -1,0 +1,62 @@
+// Host-side entry points into the sm_100a kernels (kernels.cu).
+#pragma once
+
+#include "device_types.h"
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ntrace
+{
+// Per-kernel device time of one render, measured with CUDA events on the render stream.
+struct KernelTimes
+{
+        double raygen_ms = 0;
+        double extend_ms = 0;
+        double shade_ms = 0;
+        double shadow_ms = 0;
+        long long launches = 0;
+        long long extend_launches = 0;
+        long long shadow_launches = 0;
+        long long extend_rays = 0;
+        long long shadow_rays = 0;
+};
+
+// Wavefront path pool: path state A/B (double-buffered, compacted every bounce), the hit record and
+// the shadow-ray queue, all carved out of one caller-provided device allocation.
+template <int N>
+struct Wavefront
+{
+        long long Q = 0;
+        int lights = 1;
+        float* fA = nullptr;
+        float* fB = nullptr;
+        uint32_t* pixA = nullptr;
+        uint32_t* pixB = nullptr;
+        uint32_t* smpA = nullptr;
+        uint32_t* smpB = nullptr;
+        int* lvlA = nullptr;
+        int* lvlB = nullptr;
+        float* hit_t = nullptr;
+        int* hit_obj = nullptr;
+        int* hit_facet = nullptr;
+        float* sq_f = nullptr;
+        uint32_t* sq_pix = nullptr;
+
+        static size_t bytes_for(long long Q, int lights);
+        void carve(char* base, long long Q, int lights);
+
+        // Traces total_paths camera paths starting at P.path_begin into accum (3 doubles per pixel).
+        // counters: C_COUNT device int64; host_counters: pinned host mirror of the first two.
+        // stop: optional host flag polled once per wavefront iteration (between launches).
+        cudaError_t run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
+                        unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
+                        const volatile int* stop);
+};
+
+template <int N>
+cudaError_t launch_trace_closest(const MeshDev<N>& M, const float* org, const float* dir, long long nrays, int retest,
+                                 int* facet, float* t, unsigned long long* counters, cudaStream_t st);
+}

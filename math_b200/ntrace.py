@@ -1,0 +1,317 @@
+"""Python mirror of the painter interface over the C ABI (include/ntrace.h).
+
+The reference assembles a PaintObjects<N,T> from visible shapes, light sources, a projector and the
+default surface (src/painter/objects.h:141-223) and calls paint<N,T>() (src/painter/painter.cpp:599-625).
+:class:`Scene` keeps that vocabulary: ``add_mesh`` (VisibleSharedMesh over Mesh<N,T>),
+``add_parallelotope`` (VisibleParallelotope), ``add_hyperplane_parallelotope``
+(VisibleHyperplaneParallelotope), ``add_point_light`` / ``add_constant_light``, ``set_projector``
+(Visible{Parallel,Perspective,Spherical}Projector), ``set_background`` (default surface properties),
+then ``build`` and ``render``.  Errors raise :class:`NtraceError`, carrying the library's message, as
+paint() reports through its notifier.
+
+The library is the in-tree ``libntrace.so``; there is no fallback implementation: if it cannot be
+loaded, every call raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+from pathlib import Path
+
+import numpy as np
+
+_HERE = Path(__file__).resolve().parent
+LIB_PATH = _HERE / "libntrace.so"
+
+NT_OK, NT_EINVAL, NT_EDEGENERATE, NT_ECUDA, NT_ETIMEOUT, NT_ESTOPPED, NT_ENOMEM, NT_ESTATE = range(8)
+PARALLEL, PERSPECTIVE, SPHERICAL = 0, 1, 2
+
+EXPORTED_SYMBOLS = (
+    "nt_scene_create", "nt_scene_destroy", "nt_scene_add_mesh", "nt_scene_add_parallelotope",
+    "nt_scene_add_hyperplane_parallelotope", "nt_scene_add_point_light", "nt_scene_add_constant_light",
+    "nt_scene_set_projector", "nt_scene_set_background", "nt_scene_build", "nt_scene_mesh_info", "nt_render",
+    "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
+    "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
+    "nt_scene_upload", "nt_scene_stream",
+)
+
+
+class NtraceError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"ntrace error {code}: {message}")
+        self.code = code
+
+
+class Surface(ctypes.Structure):
+    _fields_ = [("color", ctypes.c_float * 3), ("diffuse", ctypes.c_float), ("light_source", ctypes.c_int),
+                ("light_color", ctypes.c_float * 3)]
+
+
+class BuildOpts(ctypes.Structure):
+    _fields_ = [("threads", ctypes.c_int), ("host_only", ctypes.c_int)]
+
+
+class RenderOpts(ctypes.Structure):
+    _fields_ = [("samples_per_pixel", ctypes.c_int), ("max_depth", ctypes.c_int), ("seed", ctypes.c_uint64),
+                ("retest", ctypes.c_int), ("smooth_normal", ctypes.c_int), ("pool_paths", ctypes.c_int64),
+                ("timing", ctypes.c_int), ("stop", ctypes.c_void_p)]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [("paths", ctypes.c_int64), ("rays", ctypes.c_int64), ("shadow_rays", ctypes.c_int64),
+                ("facet_tests", ctypes.c_int64), ("box_steps", ctypes.c_int64), ("retests", ctypes.c_int64),
+                ("descent_levels", ctypes.c_int64), ("error_bits", ctypes.c_int64), ("spp_effective", ctypes.c_int),
+                ("seconds", ctypes.c_double), ("raygen_ms", ctypes.c_double), ("extend_ms", ctypes.c_double),
+                ("shade_ms", ctypes.c_double), ("shadow_ms", ctypes.c_double), ("launches", ctypes.c_int64),
+                ("extend_launches", ctypes.c_int64), ("shadow_launches", ctypes.c_int64),
+                ("shadow_facet_tests", ctypes.c_int64), ("shadow_box_steps", ctypes.c_int64),
+                ("shadow_retests", ctypes.c_int64), ("shadow_descent_levels", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class MeshInfo(ctypes.Structure):
+    _fields_ = [("facet_count", ctypes.c_int64), ("node_count", ctypes.c_int64), ("leaf_count", ctypes.c_int64),
+                ("index_count", ctypes.c_int64), ("max_depth", ctypes.c_int), ("distance_from_facet", ctypes.c_double),
+                ("degenerate_facets", ctypes.c_int64), ("build_seconds", ctypes.c_double),
+                ("device_bytes", ctypes.c_int64)]
+
+    def as_dict(self) -> dict:
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    """Loads libntrace.so (building it first if the sources are newer and nvcc is present)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if os.environ.get("NTRACE_NO_BUILD") != "1":
+        try:
+            from . import build as _build
+            _build.build()
+        except Exception:
+            if not LIB_PATH.exists():
+                raise
+    if not LIB_PATH.exists():
+        raise NtraceError(NT_ESTATE, f"{LIB_PATH} is missing; run math_b200/build.py")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    vp, i64, f32p, i32p = ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p
+    sig = {
+        "nt_scene_create": ([ctypes.c_int, ctypes.POINTER(vp)], ctypes.c_int),
+        "nt_scene_destroy": ([vp], ctypes.c_int),
+        "nt_scene_add_mesh": ([vp, f32p, i64, i32p, i64, ctypes.POINTER(Surface)], ctypes.c_int),
+        "nt_scene_add_parallelotope": ([vp, f32p, f32p, ctypes.POINTER(Surface)], ctypes.c_int),
+        "nt_scene_add_hyperplane_parallelotope": ([vp, f32p, f32p, ctypes.POINTER(Surface)], ctypes.c_int),
+        "nt_scene_add_point_light": ([vp, f32p, f32p, ctypes.c_float], ctypes.c_int),
+        "nt_scene_add_constant_light": ([vp, f32p, f32p], ctypes.c_int),
+        "nt_scene_set_projector": ([vp, ctypes.c_int, f32p, f32p, f32p, ctypes.c_float, i32p], ctypes.c_int),
+        "nt_scene_set_background": ([vp, ctypes.POINTER(Surface)], ctypes.c_int),
+        "nt_scene_build": ([vp, ctypes.POINTER(BuildOpts)], ctypes.c_int),
+        "nt_scene_mesh_info": ([vp, ctypes.c_int, ctypes.POINTER(MeshInfo)], ctypes.c_int),
+        "nt_render": ([vp, ctypes.POINTER(RenderOpts), ctypes.POINTER(Stats)], ctypes.c_int),
+        "nt_accum_clear": ([vp], ctypes.c_int),
+        "nt_accum_read": ([vp, f32p, ctypes.POINTER(i64)], ctypes.c_int),
+        "nt_scene_pixel_count": ([vp], i64),
+        "nt_scene_upload": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "nt_scene_stream": ([vp], vp),
+        "nt_trace_closest": ([vp, ctypes.c_int, f32p, f32p, i64, ctypes.c_int, i32p, f32p, ctypes.POINTER(Stats)],
+                             ctypes.c_int),
+        "nt_trace_closest_device": ([vp, ctypes.c_int, vp, vp, i64, ctypes.c_int, vp, vp, vp], ctypes.c_int),
+        "nt_scene_tree_export": ([vp, ctypes.c_int, i32p, i32p, f32p, f32p], ctypes.c_int),
+        "nt_last_error_message": ([], ctypes.c_char_p),
+        "nt_effective_spp": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
+        "nt_cosine_sphere_coefficient": ([ctypes.c_int], ctypes.c_double),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = lib
+    return lib
+
+
+def _check(code: int) -> None:
+    if code != NT_OK:
+        msg = library().nt_last_error_message()
+        raise NtraceError(code, msg.decode() if msg else "")
+
+
+def _f32(a, shape=None) -> np.ndarray:
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32))
+    if shape is not None:
+        arr = arr.reshape(shape)
+    return arr
+
+
+def _surface(color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False, light_color=(0.0, 0.0, 0.0)) -> Surface:
+    s = Surface()
+    for i in range(3):
+        s.color[i] = float(color[i])
+        s.light_color[i] = float(light_color[i])
+    s.diffuse = float(diffuse)
+    s.light_source = int(bool(light_source))
+    return s
+
+
+def effective_spp(n: int, spp: int) -> int:
+    return library().nt_effective_spp(n, spp)
+
+
+def cosine_sphere_coefficient(n: int) -> float:
+    return library().nt_cosine_sphere_coefficient(n)
+
+
+class Scene:
+    """One PaintObjects: objects, light sources, projector and background, in n dimensions."""
+
+    def __init__(self, n: int):
+        self.n = int(n)
+        self._lib = library()
+        h = ctypes.c_void_p()
+        _check(self._lib.nt_scene_create(self.n, ctypes.byref(h)))
+        self._h = h
+        self.screen: tuple[int, ...] = ()
+        self._keep: list = []
+
+    def close(self) -> None:
+        if self._h:
+            self._lib.nt_scene_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- assembly ----
+    def add_mesh(self, vertices, facets, color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False,
+                 light_color=(0.0, 0.0, 0.0)) -> None:
+        v = _f32(vertices).reshape(-1, self.n)
+        f = np.ascontiguousarray(np.asarray(facets, dtype=np.int32)).reshape(-1, self.n)
+        s = _surface(color, diffuse, light_source, light_color)
+        _check(self._lib.nt_scene_add_mesh(self._h, v.ctypes.data, len(v), f.ctypes.data, len(f), ctypes.byref(s)))
+
+    def add_parallelotope(self, org, edges, color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False,
+                          light_color=(0.0, 0.0, 0.0)) -> None:
+        o = _f32(org, (self.n,))
+        e = _f32(edges, (self.n, self.n))
+        s = _surface(color, diffuse, light_source, light_color)
+        _check(self._lib.nt_scene_add_parallelotope(self._h, o.ctypes.data, e.ctypes.data, ctypes.byref(s)))
+
+    def add_hyperplane_parallelotope(self, org, edges, color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False,
+                                     light_color=(0.0, 0.0, 0.0)) -> None:
+        o = _f32(org, (self.n,))
+        e = _f32(edges, (self.n - 1, self.n))
+        s = _surface(color, diffuse, light_source, light_color)
+        _check(self._lib.nt_scene_add_hyperplane_parallelotope(self._h, o.ctypes.data, e.ctypes.data, ctypes.byref(s)))
+
+    def add_point_light(self, location, rgb, unit_intensity_distance: float) -> None:
+        loc = _f32(location, (self.n,))
+        c = _f32(rgb, (3,))
+        _check(self._lib.nt_scene_add_point_light(self._h, loc.ctypes.data, c.ctypes.data,
+                                                  float(unit_intensity_distance)))
+
+    def add_constant_light(self, location, rgb) -> None:
+        loc = _f32(location, (self.n,))
+        c = _f32(rgb, (3,))
+        _check(self._lib.nt_scene_add_constant_light(self._h, loc.ctypes.data, c.ctypes.data))
+
+    def set_projector(self, kind: int, camera_org, camera_dir, screen_axes, param: float, screen_size) -> None:
+        o = _f32(camera_org, (self.n,))
+        d = _f32(camera_dir, (self.n,))
+        a = _f32(screen_axes, (self.n - 1, self.n))
+        sz = np.ascontiguousarray(np.asarray(screen_size, dtype=np.int32).reshape(self.n - 1))
+        _check(self._lib.nt_scene_set_projector(self._h, int(kind), o.ctypes.data, d.ctypes.data, a.ctypes.data,
+                                                float(param), sz.ctypes.data))
+        self.screen = tuple(int(x) for x in sz)
+
+    def set_background(self, color, light_source=False, light_color=(0.0, 0.0, 0.0)) -> None:
+        s = _surface(color, 1.0, light_source, light_color)
+        _check(self._lib.nt_scene_set_background(self._h, ctypes.byref(s)))
+
+    def build(self, threads: int = 0, host_only: bool = False) -> None:
+        o = BuildOpts(threads, int(bool(host_only)))
+        _check(self._lib.nt_scene_build(self._h, ctypes.byref(o)))
+
+    # ---- queries ----
+    def mesh_info(self, mesh_index: int = 0) -> dict:
+        info = MeshInfo()
+        _check(self._lib.nt_scene_mesh_info(self._h, mesh_index, ctypes.byref(info)))
+        return info.as_dict()
+
+    def tree_export(self, mesh_index: int = 0) -> dict:
+        info = self.mesh_info(mesh_index)
+        nodes = np.zeros((info["node_count"], 2), np.int32)
+        idx = np.zeros(max(1, info["index_count"]), np.int32)
+        sizes = np.zeros((info["max_depth"] + 1, self.n), np.float32)
+        root = np.zeros(self.n, np.float32)
+        _check(self._lib.nt_scene_tree_export(self._h, mesh_index, nodes.ctypes.data, idx.ctypes.data,
+                                              sizes.ctypes.data, root.ctypes.data))
+        return {"nodes": nodes, "indices": idx[: info["index_count"]], "level_sizes": sizes, "root_org": root,
+                "distance_from_facet": info["distance_from_facet"]}
+
+    @property
+    def pixel_count(self) -> int:
+        return int(self._lib.nt_scene_pixel_count(self._h))
+
+    @property
+    def stream(self) -> int:
+        """The scene's CUDA stream handle (as an integer)."""
+        return int(self._lib.nt_scene_stream(self._h) or 0)
+
+    def upload(self) -> int:
+        """Re-copies the scene's device arrays from the pinned host copy; returns the bytes moved."""
+        b = ctypes.c_int64()
+        _check(self._lib.nt_scene_upload(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def render(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
+               smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None) -> dict:
+        o = RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)),
+                       int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None)
+        if stop is not None:
+            o.stop = ctypes.cast(stop, ctypes.c_void_p)
+        st = Stats()
+        _check(self._lib.nt_render(self._h, ctypes.byref(o), ctypes.byref(st)))
+        return st.as_dict()
+
+    def clear(self) -> None:
+        _check(self._lib.nt_accum_clear(self._h))
+
+    def image(self) -> tuple[np.ndarray, int]:
+        """Mean colour per pixel, shape (pixels, 3), x0 fastest; and samples per pixel."""
+        out = np.zeros((self.pixel_count, 3), np.float32)
+        spp = ctypes.c_int64()
+        _check(self._lib.nt_accum_read(self._h, out.ctypes.data, ctypes.byref(spp)))
+        return out, int(spp.value)
+
+    def trace_closest(self, org, dirs, mesh_index: int = 0, retest: bool = True):
+        """Closest facet per ray (-1 = miss) and distance; plus the call's statistics."""
+        o = _f32(org).reshape(-1, self.n)
+        d = _f32(dirs).reshape(-1, self.n)
+        if o.shape != d.shape:
+            raise ValueError("org and dirs differ in shape")
+        facet = np.zeros(len(o), np.int32)
+        t = np.zeros(len(o), np.float32)
+        st = Stats()
+        _check(self._lib.nt_trace_closest(self._h, mesh_index, o.ctypes.data, d.ctypes.data, len(o), int(bool(retest)),
+                                          facet.ctypes.data, t.ctypes.data, ctypes.byref(st)))
+        return facet, t, st.as_dict()
+
+    def trace_closest_device(self, d_org: int, d_dir: int, count: int, d_facet: int, d_t: int, mesh_index: int = 0,
+                             retest: bool = True, stream: int = 0) -> None:
+        """Device-pointer variant (pointers as integers, e.g. torch tensor data_ptr())."""
+        _check(self._lib.nt_trace_closest_device(self._h, mesh_index, d_org, d_dir, count, int(bool(retest)), d_facet,
+                                                 d_t, stream or None))

@@ -1,0 +1,173 @@
+"""Scene preparation: the meshes and scenes the path tracer is measured and checked on.
+
+Mirrors the role of the reference's src/painter/scenes (single_object_scene,
+src/painter/scenes/single_object.h:102-179): a mesh of (n-1)-simplices plus, here, a floor
+parallelotope and a point light, seen through a parallel projector looking down the last axis.
+
+Meshes:
+  * ``icosphere(k)``: the icosahedron subdivided k times with vertices projected to the unit sphere
+    (k = 5 gives 20,480 triangles).
+  * ``sphere_hull(n, count, seed, cap)``: the boundary of the convex hull of ``count`` seeded points
+    uniform on the unit (n-1)-sphere (normalised Gaussian vectors, numpy PCG64 seeded with ``seed``),
+    optionally without the facets whose centroid lies within angular radius ``cap`` of +x_(n-1).  The
+    hull is computed with Qhull (scipy.spatial.ConvexHull) on the float32 points, so every facet
+    references exactly the vertices the tracer uses.
+
+A scene is a plain dict (``spec``) so that the same description feeds the product
+(:func:`build_scene`) and the checkers in ``oracle/``.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+from . import ntrace
+
+# Background: emissive, as single_object_scene's default surface (single_object.h:71-74): colour
+# for camera rays, a grey light of the colour's luminance for diffuse bounces.
+BACKGROUND = (0.30, 0.35, 0.40)
+BACKGROUND_LIGHT = (0.343, 0.343, 0.343)
+ALBEDO = 0.7
+
+
+def icosphere(subdivisions: int) -> tuple[np.ndarray, np.ndarray]:
+    t = (1.0 + math.sqrt(5.0)) / 2.0
+    verts = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+             (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    faces = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2),
+             (10, 7, 6), (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11),
+             (6, 2, 10), (8, 6, 7), (9, 8, 1)]
+    v = [np.array(p, dtype=np.float64) / np.linalg.norm(p) for p in verts]
+    cache: dict[tuple[int, int], int] = {}
+
+    def mid(a: int, b: int) -> int:
+        key = (min(a, b), max(a, b))
+        if key not in cache:
+            m = (v[a] + v[b]) / 2.0
+            v.append(m / np.linalg.norm(m))
+            cache[key] = len(v) - 1
+        return cache[key]
+
+    for _ in range(subdivisions):
+        nf = []
+        for a, b, c in faces:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        faces = nf
+    return np.array(v, dtype=np.float32), np.array(faces, dtype=np.int32)
+
+
+def sphere_points(n: int, count: int, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    p = rng.standard_normal((count, n))
+    p /= np.linalg.norm(p, axis=1, keepdims=True)
+    return p.astype(np.float32)
+
+
+def sphere_hull(n: int, count: int, seed: int, cap: float | None = None) -> tuple[np.ndarray, np.ndarray]:
+    from scipy.spatial import ConvexHull
+
+    pts = sphere_points(n, count, seed)
+    facets = ConvexHull(pts.astype(np.float64)).simplices.astype(np.int32)
+    if cap is not None:
+        centroid = pts[facets].astype(np.float64).mean(axis=1)
+        centroid /= np.linalg.norm(centroid, axis=1, keepdims=True)
+        keep = centroid[:, n - 1] < math.cos(cap)
+        facets = facets[keep]
+    used = np.unique(facets)
+    remap = np.full(len(pts), -1, np.int32)
+    remap[used] = np.arange(len(used), dtype=np.int32)
+    return np.ascontiguousarray(pts[used]), np.ascontiguousarray(remap[facets])
+
+
+def floor_slab(n: int) -> tuple[np.ndarray, np.ndarray]:
+    """[-4,4]^(n-1) x [-1.1,-1]."""
+    org = np.full(n, -4.0, np.float32)
+    org[n - 1] = -1.1
+    edges = np.diag(np.full(n, 8.0, np.float32))
+    edges[n - 1, n - 1] = 0.1
+    return org, edges.astype(np.float32)
+
+
+def make_spec(n: int, verts: np.ndarray | None, facets: np.ndarray | None, screen: int, spp: int, max_depth: int = 5,
+              seed: int = 0, floor: bool = True, extent: float = 8.0, light_kind: int = 0,
+              projector: int = ntrace.PARALLEL) -> dict:
+    """A floor scene: mesh, floor slab, one light at (2, ..., 2, 3), parallel projection of
+    [-extent/2, extent/2]^(n-1) seen from +x_(n-1)."""
+    light = np.full(n, 2.0, np.float32)
+    light[n - 1] = 3.0
+    cam = np.zeros(n, np.float32)
+    cam[n - 1] = 10.0
+    cdir = np.zeros(n, np.float32)
+    cdir[n - 1] = -1.0
+    axes = np.eye(n, dtype=np.float32)[: n - 1]
+    spec = {
+        "n": n,
+        "verts": verts,
+        "facets": facets,
+        "mesh_color": (ALBEDO, ALBEDO, ALBEDO),
+        "mesh_diffuse": 1.0,
+        "floor": None,
+        "light": {"kind": light_kind, "pos": light, "color": (1.0, 1.0, 1.0),
+                  "unit": float(np.linalg.norm(light.astype(np.float64)))},
+        "projector": {"kind": projector, "org": cam, "dir": cdir, "axes": axes,
+                      "param": extent / screen if projector == ntrace.PARALLEL else 60.0,
+                      "screen": [screen] * (n - 1)},
+        "bg": {"color": BACKGROUND, "light": True, "light_color": BACKGROUND_LIGHT},
+        "spp": spp,
+        "max_depth": max_depth,
+        "seed": seed,
+    }
+    if floor:
+        org, edges = floor_slab(n)
+        spec["floor"] = {"org": org, "edges": edges, "color": (ALBEDO, ALBEDO, ALBEDO), "diffuse": 1.0}
+    return spec
+
+
+def config(name: str) -> dict:
+    """The measured configurations (full size) and their reduced test-size counterparts."""
+    if name == "n3":
+        v, f = icosphere(5)
+        return make_spec(3, v, f, screen=400, spp=16)
+    if name == "n4":
+        v, f = sphere_hull(4, 100_000, seed=0)
+        return make_spec(4, v, f, screen=128, spp=16)
+    if name == "n5":
+        v, f = sphere_hull(5, 50_000, seed=0, cap=0.5)
+        return make_spec(5, v, f, screen=48, spp=4)
+    if name == "n3_small":
+        v, f = icosphere(2)
+        return make_spec(3, v, f, screen=48, spp=16)
+    if name == "n4_small":
+        v, f = sphere_hull(4, 800, seed=1)
+        return make_spec(4, v, f, screen=12, spp=8)
+    if name == "n5_small":
+        v, f = sphere_hull(5, 300, seed=2, cap=0.5)
+        return make_spec(5, v, f, screen=6, spp=4)
+    if name == "n6_small":
+        v, f = sphere_hull(6, 120, seed=3)
+        return make_spec(6, v, f, screen=4, spp=2)
+    raise KeyError(name)
+
+
+def build_scene(spec: dict, threads: int = 0) -> ntrace.Scene:
+    n = spec["n"]
+    s = ntrace.Scene(n)
+    if spec["verts"] is not None:
+        s.add_mesh(spec["verts"], spec["facets"], color=spec["mesh_color"], diffuse=spec["mesh_diffuse"])
+    if spec["floor"] is not None:
+        fl = spec["floor"]
+        s.add_parallelotope(fl["org"], fl["edges"], color=fl["color"], diffuse=fl["diffuse"])
+    L = spec["light"]
+    if L["kind"] == 0:
+        s.add_point_light(L["pos"], L["color"], L["unit"])
+    else:
+        s.add_constant_light(L["pos"], L["color"])
+    P = spec["projector"]
+    s.set_projector(P["kind"], P["org"], P["dir"], P["axes"], P["param"], P["screen"])
+    bg = spec["bg"]
+    s.set_background(bg["color"], bg["light"], bg["light_color"])
+    s.build(threads)
+    return s

@@ -3,9 +3,11 @@
  * TEST INFRASTRUCTURE ONLY: loaded by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg
  * as the checker; never linked into or called by the product.  See ntrace_oracle.h.
  */
-#define _POSIX_C_SOURCE 200809L
+#define _GNU_SOURCE
 
 #include "ntrace_oracle.h"
+
+#include <unistd.h>
 
 #include <float.h>
 #include <math.h>
@@ -419,6 +421,7 @@ static double now_seconds(void)
                         total *= in->screen[j];                                                                   \
                 }                                                                                                 \
                 job.npix = pixels ? npix : total;                                                                 \
+                job.total_pixels = total;                                                                         \
                 job.sample_offset = sample_offset;                                                                \
                 job.out = rgb_out;                                                                                \
                 pthread_mutex_init(&job.lock, NULL);                                                              \

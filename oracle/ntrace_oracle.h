@@ -93,7 +93,8 @@ int ort_mesh_facet_export(void* mesh, double* normal, double* planes);
 
 /* Path tracing (paint<N,T>) with the Philox stream.  pixels == NULL: whole screen, rgb_out dense
  * (x0 fastest); otherwise the listed pixels.  sample_offset shifts the sample index (progressive
- * passes): sample s of a pixel uses path id = pixel * spp_eff + sample_offset + s. */
+ * passes): sample s of pixel p (linear index, x0 fastest) uses
+ * path id = (sample_offset + s) * pixel_count + p. */
 int ort_paint(const ort_scene* scene, int spp, int max_depth, uint64_t seed, int threads, const int* pixels,
               long npix, long long sample_offset, float* rgb_out, ort_stats* stats, char* err, int errlen);
 
