@@ -335,6 +335,120 @@ __device__ __noinline__ bool find_leaf_dfs(const MeshDev<N>& M, const float* p, 
         return false;
 }
 
+// The root-to-leaf path of the previous point location of the same walk.  Consecutive leaves of a
+// walk share most of their ancestors; the child chosen at each level depends only on the point and
+// the box origins above it, so while the new point picks the same children the node records are
+// known and are not read again.  The leaf found is the one a full descent finds.
+struct PathCache
+{
+        int depth;                 // level of the cached leaf; -1: empty
+        unsigned long long bits;   // child index chosen at each level, 6 bits per level
+        int2 leaf;                 // the cached leaf's record
+        int leaf_node;
+        int fc[MAX_LEVELS];        // first child of the internal node at each level of the path
+};
+
+template <int N>
+__device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const float* p, PathCache& pc, Leaf<N>* out,
+                                                 int2* leaf_rec, long long* descent)
+{
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+        {
+                if (!(p[i] <= M.root_d1[i]) || !(-p[i] <= -M.root_org[i]))
+                {
+                        return false;
+                }
+        }
+        float o[N];
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+        {
+                o[i] = M.root_org[i];
+        }
+        int node = 0;
+        bool ambiguous = false;
+        bool same = pc.depth >= 0;
+        for (int lvl = 0; lvl < MAX_LEVELS; ++lvl)
+        {
+                int2 nd;
+                if (same)
+                {
+                        nd = (lvl == pc.depth) ? pc.leaf : make_int2(pc.fc[lvl], -1);
+                }
+                else
+                {
+                        nd = __ldg(&M.nodes[node]);
+                }
+                ++*descent;
+                if (nd.y >= 0)
+                {
+                        out->node = node;
+                        out->level = lvl;
+#pragma unroll
+                        for (int i = 0; i < N; ++i)
+                        {
+                                out->org[i] = o[i];
+                        }
+                        *leaf_rec = nd;
+                        pc.depth = lvl;
+                        pc.leaf = nd;
+                        pc.leaf_node = node;
+                        return true;
+                }
+                if (!same)
+                {
+                        pc.fc[lvl] = nd.x;
+                }
+                int child = 0;
+                bool fail = false;
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        float h = M.size[lvl + 1][i];
+                        float mid = o[i] + h;
+                        bool lo_ok = p[i] <= mid;
+                        bool hi_ok = (-p[i] <= -mid) && (p[i] <= mid + h);
+                        if (lo_ok)
+                        {
+                                ambiguous |= hi_ok;
+                        }
+                        else if (hi_ok)
+                        {
+                                child |= 1 << i;
+                                o[i] = mid;
+                        }
+                        else
+                        {
+                                fail = true;
+                        }
+                }
+                if (fail)
+                {
+                        pc.depth = -1;
+                        if (ambiguous)
+                        {
+                                bool found = find_leaf_dfs<N>(M, p, out);
+                                if (found)
+                                {
+                                        *leaf_rec = __ldg(&M.nodes[out->node]);
+                                }
+                                return found;
+                        }
+                        return false;
+                }
+                const int shift = 6 * lvl;
+                if (same && (int)((pc.bits >> shift) & 63ull) != child)
+                {
+                        same = false;
+                }
+                pc.bits = (pc.bits & ~(63ull << shift)) | ((unsigned long long)child << shift);
+                node = nd.x + child;
+        }
+        pc.depth = -1;
+        return false;
+}
+
 template <int N>
 __device__ __forceinline__ bool find_leaf(const MeshDev<N>& M, const float* p, Leaf<N>* out, long long* descent)
 {
@@ -419,9 +533,12 @@ template <int N>
 __device__ __forceinline__ int facet_test32(const float4* rec, const Ray<N>& r, float ao, float* t_out)
 {
         constexpr float EPS = 5.9604645e-08f;  // 2^-24
+        // the record is read in stages: the plane of the simplex first, each barycentric plane only
+        // when the tests before it have not already rejected the facet
+        constexpr int HEAD4 = (Rec32<N>::OFF_PLANES + 3) / 4;
         float f[Rec32<N>::FLOATS];
 #pragma unroll
-        for (int q = 0; q < Rec32<N>::F4; ++q)
+        for (int q = 0; q < HEAD4; ++q)
         {
                 float4 v = __ldg(rec + q);
                 f[4 * q + 0] = v.x;
@@ -463,6 +580,17 @@ __device__ __forceinline__ int facet_test32(const float4* rec, const Ray<N>& r, 
 #pragma unroll
         for (int i = 0; i < N - 1; ++i)
         {
+                const int first4 = (i == 0) ? HEAD4 : (Rec32<N>::OFF_PLANES + i * (N + 1) + 3) / 4;
+                const int need4 = (Rec32<N>::OFF_PLANES + (i + 1) * (N + 1) + 3) / 4;
+#pragma unroll
+                for (int q = first4; q < need4; ++q)
+                {
+                        float4 v = __ldg(rec + q);
+                        f[4 * q + 0] = v.x;
+                        f[4 * q + 1] = v.y;
+                        f[4 * q + 2] = v.z;
+                        f[4 * q + 3] = v.w;
+                }
                 const float* pl = f + Rec32<N>::OFF_PLANES + i * (N + 1);
                 float b = vdot<N>(p, pl) - pl[N];
                 if (b <= -e_b || b >= 1.0f + e_b)
@@ -603,6 +731,16 @@ struct WalkStats
         int error;
 };
 
+// FP64 re-test of one facet, kept out of line so that its double-precision state does not occupy
+// registers of the hot FP32 walk.
+template <int N>
+__device__ __noinline__ bool retest_facet(const double* rec, const Ray<N>& ray, const Ray64Source<N>& src, double* t)
+{
+        Ray64<N> r64;
+        src.get(ray, &r64);
+        return facet_test64<N>(rec, r64, t);
+}
+
 // Closest facet of one leaf (ray_intersection over indices, ray_intersection.h:134-159: strict <
 // in list order).  Returns the facet or -1 and its distance.
 template <int N>
@@ -613,8 +751,6 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
         float bt = FLT_MAX;
         double bt64 = 0;
         bool b64 = false;
-        bool have64 = false;
-        Ray64<N> r64;
         for (int q = 0; q < leaf.y; ++q)
         {
                 int f = __ldg(&M.leaf_idx[leaf.x + q]);
@@ -641,12 +777,7 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
                         else
                         {
                                 ++ws->retests;
-                                if (!have64)
-                                {
-                                        src.get(ray, &r64);
-                                        have64 = true;
-                                }
-                                if (!facet_test64<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, r64, &t64))
+                                if (!retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, src, &t64))
                                 {
                                         continue;
                                 }
@@ -659,15 +790,10 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
                 float tol = 1e-5f * (fabsf(t) + ao) + 1e-30f;
                 if (retest && best >= 0 && fabsf(t - bt) <= tol)
                 {
-                        if (!have64)
-                        {
-                                src.get(ray, &r64);
-                                have64 = true;
-                        }
                         if (!is64)
                         {
                                 ++ws->retests;
-                                if (!facet_test64<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, r64, &t64))
+                                if (!retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, src, &t64))
                                 {
                                         continue;
                                 }
@@ -677,7 +803,7 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
                         {
                                 ++ws->retests;
                                 double tb;
-                                if (facet_test64<N>(M.rec64 + (size_t)best * Rec64<N>::DOUBLES, r64, &tb))
+                                if (retest_facet<N>(M.rec64 + (size_t)best * Rec64<N>::DOUBLES, ray, src, &tb))
                                 {
                                         bt64 = tb;
                                         b64 = true;
@@ -733,12 +859,16 @@ __device__ bool mesh_closest(const MeshDev<N>& M, const Ray<N>& ray, float root_
         }
         float travelled = 0;
         bool first = true;
+        PathCache pc;
+        pc.depth = -1;
+        pc.bits = 0;
         // a ray crosses at most (boxes per axis) x N leaves of a 2^N-tree at most 2^9 boxes wide;
         // the bound leaves ample margin and turns a walk that does not advance into an error flag
         for (int step = 0; step < 16384; ++step)
         {
                 Leaf<N> lf;
-                if (find_leaf<N>(M, probe, &lf, &ws->descent))
+                int2 nd;
+                if (find_leaf_cached<N>(M, probe, pc, &lf, &nd, &ws->descent))
                 {
                         ++ws->box_steps;
                         const float* sz = M.size[lf.level];
@@ -746,7 +876,6 @@ __device__ bool mesh_closest(const MeshDev<N>& M, const Ray<N>& ray, float root_
                         {
                                 return false;
                         }
-                        int2 nd = __ldg(&M.nodes[lf.node]);
                         if (nd.y > 0)
                         {
                                 float t;

@@ -164,6 +164,9 @@ enum Counter : int
         C_SH_BOX_STEPS = 10,
         C_SH_DESCENT = 11,
         C_SH_RETESTS = 12,
+        // work cursors of the persistent extension and shadow kernels
+        C_WORK_EXT = 13,
+        C_WORK_SH = 14,
         C_COUNT = 16
 };
 

@@ -11,6 +11,8 @@ namespace ntrace
 namespace
 {
 constexpr int BLOCK = 256;
+// resident blocks per SM asked of the tree-walk kernels (caps their registers at 65536 / (3 x 256))
+constexpr int WALK_MIN_BLOCKS = 3;
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -103,6 +105,17 @@ __global__ void __launch_bounds__(BLOCK) k_trace_closest(__grid_constant__ const
                         {
                                 f = -1;
                                 t = 0;
+                        }
+                        else if (retest)
+                        {
+                                // report the distance of the chosen facet in FP64 (rounded once)
+                                Ray64<N> r64;
+                                src.get(r, &r64);
+                                double t64;
+                                if (facet_test64<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, r64, &t64))
+                                {
+                                        t = (float)t64;
+                                }
                         }
                 }
                 facet_out[i] = f;
@@ -215,36 +228,53 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevSce
         A.level[slot] = 0;
 }
 
+// Persistent warps take 32 consecutive rays at a time from a device counter until the queue is
+// exhausted: no block waits for another block's slowest ray, and the grid is sized to the SMs.
+__device__ __forceinline__ long long warp_take(unsigned long long* work)
+{
+        long long base = 0;
+        if ((threadIdx.x & 31) == 0)
+        {
+                base = (long long)atomicAdd(work, 32ull);
+        }
+        return __shfl_sync(0xffffffffu, base, 0);
+}
+
 // extension: closest object per path (ray_intersection over objects, ray_intersection.h:26-105)
 template <int N>
-__global__ void __launch_bounds__(BLOCK) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, long long count,
+__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, long long count,
                                                   unsigned long long* counters)
 {
-        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         WalkStats ws{0, 0, 0, 0, 0};
-        if (i < count)
+        long long rays = 0;
+        for (long long base = warp_take(counters + C_WORK_EXT); base < count; base = warp_take(counters + C_WORK_EXT))
         {
-                Ray<N> r;
+                long long i = base + (threadIdx.x & 31);
+                if (i < count)
+                {
+                        Ray<N> r;
 #pragma unroll
-                for (int k = 0; k < N; ++k)
-                {
-                        r.org[k] = A.at(k, i);
-                        r.dir[k] = A.at(N + k, i);
-                }
-                float t;
-                int obj, facet;
-                if (scene_closest<N>(S, r, &t, &obj, &facet, &ws))
-                {
-                        H.t[i] = t;
-                        H.obj[i] = obj;
-                        H.facet[i] = facet;
-                }
-                else
-                {
-                        H.obj[i] = -1;
+                        for (int k = 0; k < N; ++k)
+                        {
+                                r.org[k] = A.at(k, i);
+                                r.dir[k] = A.at(N + k, i);
+                        }
+                        float t;
+                        int obj, facet;
+                        if (scene_closest<N>(S, r, &t, &obj, &facet, &ws))
+                        {
+                                H.t[i] = t;
+                                H.obj[i] = obj;
+                                H.facet[i] = facet;
+                        }
+                        else
+                        {
+                                H.obj[i] = -1;
+                        }
+                        ++rays;
                 }
         }
-        flush_stats<false>(counters, ws, i < count ? 1 : 0, 0);
+        flush_stats<false>(counters, ws, rays, 0);
 }
 
 __device__ __forceinline__ void accumulate(double* accum, uint32_t pixel, float r, float g, float b)
@@ -477,33 +507,50 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
 
 // shadow rays: light_source_is_visible (painter.cpp:172-186); visible -> add the light's share
 template <int N>
-__global__ void __launch_bounds__(BLOCK) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, long long count,
+__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, long long count,
                                                   unsigned long long* counters)
 {
-        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         WalkStats ws{0, 0, 0, 0, 0};
-        if (i < count)
+        long long rays = 0;
+        for (long long base = warp_take(counters + C_WORK_SH); base < count; base = warp_take(counters + C_WORK_SH))
         {
-                Ray<N> r;
+                long long i = base + (threadIdx.x & 31);
+                if (i < count)
+                {
+                        Ray<N> r;
 #pragma unroll
-                for (int k = 0; k < N; ++k)
-                {
-                        r.org[k] = SQ.at(k, i);
-                        r.dir[k] = SQ.at(N + k, i);
-                }
-                float tmax = SQ.at(2 * N, i);
-                if (scene_visible<N>(S, r, tmax, &ws))
-                {
-                        accumulate(accum, SQ.pix[i], SQ.at(2 * N + 1, i), SQ.at(2 * N + 2, i), SQ.at(2 * N + 3, i));
+                        for (int k = 0; k < N; ++k)
+                        {
+                                r.org[k] = SQ.at(k, i);
+                                r.dir[k] = SQ.at(N + k, i);
+                        }
+                        float tmax = SQ.at(2 * N, i);
+                        if (scene_visible<N>(S, r, tmax, &ws))
+                        {
+                                accumulate(accum, SQ.pix[i], SQ.at(2 * N + 1, i), SQ.at(2 * N + 2, i), SQ.at(2 * N + 3, i));
+                        }
+                        ++rays;
                 }
         }
-        flush_stats<true>(counters, ws, 0, i < count ? 1 : 0);
+        flush_stats<true>(counters, ws, 0, rays);
 }
 
 template <int N>
 long long grid_for(long long count)
 {
         return (count + BLOCK - 1) / BLOCK;
+}
+
+// Resident blocks of a persistent kernel on this device (all SMs, as many blocks per SM as its
+// registers and shared memory allow).
+template <typename K>
+long long resident_blocks(K kernel)
+{
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, 0);
+        return (long long)std::max(1, sms) * std::max(1, per_sm);
 }
 }
 
@@ -548,13 +595,12 @@ void Wavefront<N>::carve(char* base, long long Q, int lights)
 template <int N>
 cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
                               unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
-                              const volatile int* stop)
+                              bool timing, const volatile int* stop)
 {
         long long active = 0;
         long long next = 0;
         bool flip = false;
         cudaEvent_t ev[8];
-        const bool timing = times != nullptr;
         if (timing)
         {
                 for (auto& e : ev)
@@ -563,6 +609,8 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                 }
         }
         const long long path_base = P.path_begin;
+        static const long long extend_blocks = resident_blocks(k_extend<N>);
+        static const long long shadow_blocks = resident_blocks(k_shadow<N>);
         for (int iter = 0; active > 0 || next < total_paths; ++iter)
         {
                 if (stop && *stop)
@@ -593,7 +641,9 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                 {
                         cudaEventRecord(ev[1], st);
                 }
-                k_extend<N><<<(unsigned)grid_for<N>(active), BLOCK, 0, st>>>(S, A, H, active, counters);
+                cudaMemsetAsync(counters + C_WORK_EXT, 0, 2 * sizeof(unsigned long long), st);
+                k_extend<N><<<(unsigned)std::min(extend_blocks, grid_for<N>(active)), BLOCK, 0, st>>>(S, A, H, active,
+                                                                                                      counters);
                 if (timing)
                 {
                         cudaEventRecord(ev[2], st);
@@ -615,7 +665,8 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                 long long shadows = (long long)host_counters[C_SHADOW];
                 if (shadows > 0)
                 {
-                        k_shadow<N><<<(unsigned)grid_for<N>(shadows), BLOCK, 0, st>>>(S, SQ, accum, shadows, counters);
+                        k_shadow<N><<<(unsigned)std::min(shadow_blocks, grid_for<N>(shadows)), BLOCK, 0, st>>>(
+                                S, SQ, accum, shadows, counters);
                 }
                 if (timing)
                 {
@@ -630,12 +681,12 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                         times->shade_ms += ms;
                         cudaEventElapsedTime(&ms, ev[3], ev[4]);
                         times->shadow_ms += ms;
-                        times->extend_launches += 1;
-                        times->shadow_launches += shadows > 0 ? 1 : 0;
-                        times->launches += (fresh > 0 ? 1 : 0) + 2 + (shadows > 0 ? 1 : 0);
-                        times->extend_rays += active;
-                        times->shadow_rays += shadows;
                 }
+                times->extend_launches += 1;
+                times->shadow_launches += shadows > 0 ? 1 : 0;
+                times->launches += (fresh > 0 ? 1 : 0) + 2 + (shadows > 0 ? 1 : 0);
+                times->extend_rays += active;
+                times->shadow_rays += shadows;
                 active = survivors;
                 flip = !flip;
         }

@@ -50,10 +50,11 @@ struct Wavefront
 
         // Traces total_paths camera paths starting at P.path_begin into accum (3 doubles per pixel).
         // counters: C_COUNT device int64; host_counters: pinned host mirror of the first two.
-        // stop: optional host flag polled once per wavefront iteration (between launches).
+        // times: launch counts always, per-kernel device times when timing (events around every
+        // launch); stop: optional host flag polled once per wavefront iteration (between launches).
         cudaError_t run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
                         unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
-                        const volatile int* stop);
+                        bool timing, const volatile int* stop);
 };
 
 template <int N>

@@ -1213,7 +1213,7 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st)
         check_cuda(cudaMemsetAsync(s->counters.p, 0, s->counters.bytes, s->stream), "memset counters");
         KernelTimes times;
         cudaError_t e = W.run(S, P, s->accum.as<double>(), s->counters.as<unsigned long long>(), s->host_counters, total,
-                              s->stream, o.timing ? &times : nullptr, o.stop);
+                              s->stream, &times, o.timing != 0, o.stop);
         check_cuda(e, "render");
         check_cuda(cudaMemcpyAsync(s->host_counters, s->counters.p, C_COUNT * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, s->stream),
