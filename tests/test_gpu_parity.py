@@ -63,8 +63,42 @@ def _edge_rays(verts, facets, count, seed):
     return org.astype(np.float32), (target - org).astype(np.float32)
 
 
+def _exact_hit(verts, facet_vertices, org, direction):
+    """Exact rational intersection of the ray org + t * unit(direction) with the simplex: returns t if
+    the intersection lies strictly inside the simplex with t > 0, else None.  The unit direction is
+    taken as its double-precision value (as the FP64 reference computes it)."""
+    from fractions import Fraction as F
+
+    n = len(org)
+    d = np.asarray(direction, np.float64)
+    d = d / np.linalg.norm(d)
+    V = [[F(float(x)) for x in verts[i]] for i in facet_vertices]
+    # unknowns b_0..b_(n-1), t: sum b_j V_j - t d = org, sum b_j = 1
+    rows = [[V[j][k] for j in range(n)] + [-F(float(d[k]))] + [F(float(org[k]))] for k in range(n)]
+    rows.append([F(1)] * n + [F(0), F(1)])
+    m = n + 1
+    for c in range(m):
+        piv = next((r for r in range(c, m) if rows[r][c] != 0), None)
+        if piv is None:
+            return None
+        rows[c], rows[piv] = rows[piv], rows[c]
+        for r in range(m):
+            if r != c and rows[r][c] != 0:
+                f = rows[r][c] / rows[c][c]
+                rows[r] = [a - f * b for a, b in zip(rows[r], rows[c])]
+    sol = [rows[r][m] / rows[r][r] for r in range(m)]
+    if all(b > 0 for b in sol[:n]) and sol[n] > 0:
+        return sol[n]
+    return None
+
+
 @pytest.mark.parametrize("n,points", [(3, 2000), (4, 1500), (5, 400)])
 def test_closest_hit_bit_exact_against_oracle_fresh_rays(require_gpu, port, n, points):
+    """Fresh ray sets (20,000 random, 20,000 aimed at facet boundaries) against the FP64 oracle.  Where
+    the two differ, the FP64 oracle must be the one in the wrong: its double-precision tree can leave a
+    facet out of a leaf that the facet crosses (Mesh<N,double>'s box-simplex test, reproduced exactly by
+    the oracle), so it misses the true first hit; exact rational arithmetic then shows the GPU's facet is
+    hit, and nearer than the oracle's."""
     from math_b200 import scenes
 
     verts, facets = scenes.sphere_hull(n, points, seed=40 + n)
@@ -78,9 +112,17 @@ def test_closest_hit_bit_exact_against_oracle_fresh_rays(require_gpu, port, n, p
     facet, t, st = s.trace_closest(org, dirs, retest=True)
     pf, pt, _ = port.trace(port.mesh(n, verts, facets, dbl=True), org, dirs)
     assert st["error_bits"] == 0
-    assert np.array_equal(facet, pf), int((facet != pf).sum())
-    hit = facet >= 0
-    assert np.allclose(t[hit], pt[hit], rtol=2e-6, atol=0)
+    bad = np.nonzero(facet != pf)[0]
+    assert len(bad) <= 1e-4 * len(org)
+    for i in bad:
+        assert facet[i] >= 0
+        t_gpu = _exact_hit(verts, facets[facet[i]], org[i], dirs[i])
+        assert t_gpu is not None, i
+        if pf[i] >= 0:
+            t_oracle = _exact_hit(verts, facets[pf[i]], org[i], dirs[i])
+            assert t_oracle is None or t_gpu < t_oracle, i
+    same = (facet == pf) & (facet >= 0)
+    assert np.allclose(t[same], pt[same], rtol=2e-6, atol=0)
 
 
 @pytest.mark.parametrize("name", ["n3_small", "n4_small", "n5_small", "n6_small"])
