@@ -155,6 +155,27 @@ int nt_scene_mesh_info(nt_scene* scene, int mesh_index, nt_mesh_info* info);
  * of the screen, added to the scene's accumulator; successive calls continue the sample sequence. */
 int nt_render(nt_scene* scene, const nt_render_opts* opts, nt_stats* stats);
 
+/* nt_render for callers that cannot allocate device memory: applications that own all device memory
+ * through their own allocator or a budget fixed at start-up, plugins inside such hosts, and frame
+ * loops where an allocation (which may synchronise the device or fail) is not allowed.  No counterpart
+ * in the reference, whose painter runs on host memory.
+ *
+ * One pass of samples_per_pixel over the built scene, like nt_render, but the wavefront's working
+ * memory is one file-scope device array of NT_NOALLOC_SCRATCH_BYTES inside the library, and the pass's
+ * per-pixel sums (red, green, blue as doubles, x0 fastest) are ADDED to the caller's d_accum
+ * (pixel_count x 3 doubles of device memory; zero it before the first pass).  sample_offset is the
+ * index of the pass's first sample per pixel (0, then the effective samples of the passes before).
+ * stream: a cudaStream_t, NULL for the scene's stream.  The call allocates nothing: no cudaMalloc,
+ * cudaFree, cudaMallocHost, stream or event; its first call on a device looks up the array's device
+ * address (cudaGetSymbolAddress) for that device, so make that first call before any stream capture.
+ * The array holds at most the path pool that fits in it: opts->pool_paths above that capacity is
+ * rejected with NT_EINVAL (0 uses the capacity).  Every GPU that loads the library keeps the array
+ * until the process exits; all calls share it and it keeps the last call's contents (each call clears
+ * its counters), so calls that overlap on the GPU race and must be serialised by the caller. */
+#define NT_NOALLOC_SCRATCH_BYTES (64u << 20)
+int nt_render_noalloc(nt_scene* scene, const nt_render_opts* opts, double* d_accum, int64_t sample_offset,
+                      void* stream, nt_stats* stats);
+
 int nt_accum_clear(nt_scene* scene);
 
 /* Mean colour per pixel (pixel_count x 3 floats, x0 fastest) and the samples behind it. */

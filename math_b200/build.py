@@ -74,9 +74,17 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
-    if force or _stale(LIB, [cu_obj, cpp_obj]):
-        cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj), "-Xlinker",
-               "--no-undefined", "-lpthread"]
+    noalloc = CSRC / "noalloc.cu"
+    noalloc_obj = BUILD_DIR / "noalloc.o"
+    if force or _stale(noalloc_obj, [noalloc] + headers):
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *common, "-c", str(noalloc), "-o",
+               str(noalloc_obj)]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj]):
+        cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj),
+               str(noalloc_obj), "-Xlinker", "--no-undefined", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

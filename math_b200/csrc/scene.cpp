@@ -1256,6 +1256,127 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st)
         }
 }
 
+// One pass of the wavefront on caller-provided working memory (nt_render_noalloc): the scratch holds
+// the device counters (first 256 bytes) and the path pool; the pass's sums are added to d_accum.
+template <int N>
+void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long long sample_offset, cudaStream_t st,
+                    void* scratch, size_t scratch_bytes, nt_stats* out)
+{
+        auto t0 = std::chrono::steady_clock::now();
+        if (o.samples_per_pixel < 1)
+        {
+                fail(NT_EINVAL, "Stratified jittered sample count is not a positive integer");
+        }
+        if (o.max_depth < 0)
+        {
+                fail(NT_EINVAL, "max_depth must be >= 0");
+        }
+        if (!d_accum)
+        {
+                fail(NT_EINVAL, "the accumulator is NULL");
+        }
+        if (sample_offset < 0)
+        {
+                fail(NT_EINVAL, "sample_offset must be >= 0");
+        }
+        const int k = one_dimension_size(N, o.samples_per_pixel);
+        long long spp_eff = 1;
+        for (int i = 0; i < N - 1; ++i)
+        {
+                spp_eff *= k;
+        }
+        const long long npix = s->pixel_count();
+        const long long total = npix * spp_eff;
+        if ((sample_offset + spp_eff) * npix >= (1ll << 62) || sample_offset + spp_eff > 0xffffffffll)
+        {
+                fail(NT_EINVAL, "sample count overflow");
+        }
+        const int lights = (int)s->lights.size();
+        const size_t fixed = Wavefront<N>::bytes_for(0, lights);
+        const size_t per_path = Wavefront<N>::bytes_for(1, lights) - fixed;
+        const size_t head = 256;  // device counters
+        const long long capacity =
+                scratch_bytes > head + fixed ? (long long)((scratch_bytes - head - fixed) / per_path) : 0;
+        if (capacity < 256)
+        {
+                fail(NT_EINVAL, "the no-alloc scratch is too small for this scene");
+        }
+        if (o.pool_paths > capacity)
+        {
+                fail(NT_EINVAL, "pool_paths " + std::to_string(o.pool_paths) + " exceeds the no-alloc scratch capacity of " +
+                                        std::to_string(capacity) + " paths (n = " + std::to_string(N) + ", " +
+                                        std::to_string(lights) + " light(s), " + std::to_string(scratch_bytes) +
+                                        " bytes)");
+        }
+        long long Q = o.pool_paths > 0 ? o.pool_paths : capacity;
+        Q = std::max<long long>(1, std::min(Q, total));
+        DevScene<N> S;
+        std::memcpy(&S, s->dev_scene.data(), sizeof(S));
+        S.max_depth = o.max_depth;
+        S.retest = o.retest;
+        S.smooth_normal = o.smooth_normal;
+        unsigned long long* counters = static_cast<unsigned long long*>(scratch);
+        Wavefront<N> W;
+        W.carve(static_cast<char*>(scratch) + head, Q, lights);
+        PassDev P{};
+        P.key0 = (uint32_t)o.seed;
+        P.key1 = (uint32_t)(o.seed >> 32);
+        P.spp_eff = (int)spp_eff;
+        P.k1d = k;
+        P.recip_k = 1.0f / k;
+        P.npix = npix;
+        P.sample_offset = sample_offset;
+        P.path_begin = 0;
+        P.path_end = total;
+        check_cuda(cudaMemsetAsync(counters, 0, C_COUNT * sizeof(unsigned long long), st), "memset counters");
+        unsigned long long host_counters[C_COUNT] = {};
+        KernelTimes times;
+        check_cuda(W.run(S, P, d_accum, counters, host_counters, total, st, &times, false, o.stop), "render");
+        check_cuda(cudaMemcpyAsync(host_counters, counters, C_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
+                   "counters");
+        check_cuda(cudaStreamSynchronize(st), "render sync");
+        bool stopped = o.stop && *o.stop;
+        if (out)
+        {
+                std::memset(out, 0, sizeof(*out));
+                out->paths = total;
+                out->rays = (int64_t)host_counters[C_RAYS];
+                out->shadow_rays = (int64_t)host_counters[C_SHADOW_RAYS];
+                out->facet_tests = (int64_t)host_counters[C_FACET_TESTS];
+                out->box_steps = (int64_t)host_counters[C_BOX_STEPS];
+                out->retests = (int64_t)host_counters[C_RETESTS];
+                out->descent_levels = (int64_t)host_counters[C_DESCENT];
+                out->error_bits = (int64_t)host_counters[C_ERROR];
+                out->spp_effective = (int)spp_eff;
+                out->launches = times.launches;
+                out->extend_launches = times.extend_launches;
+                out->shadow_launches = times.shadow_launches;
+                out->shadow_facet_tests = (int64_t)host_counters[C_SH_FACET_TESTS];
+                out->shadow_box_steps = (int64_t)host_counters[C_SH_BOX_STEPS];
+                out->shadow_retests = (int64_t)host_counters[C_SH_RETESTS];
+                out->shadow_descent_levels = (int64_t)host_counters[C_SH_DESCENT];
+                out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        }
+        if (stopped)
+        {
+                fail(NT_ESTOPPED, "render stopped");
+        }
+        if (host_counters[C_ERROR])
+        {
+                fail(NT_ETIMEOUT, "a bounded device loop ran out (error bits " + std::to_string(host_counters[C_ERROR]) + ")");
+        }
+}
+
+template <int N>
+struct NoallocF
+{
+        static void run(nt_scene* s, const nt_render_opts& o, double* acc, long long off, cudaStream_t st, void* scratch,
+                        size_t bytes, nt_stats* out)
+        {
+                render_noalloc<N>(s, o, acc, off, st, scratch, bytes, out);
+        }
+};
+
 template <int N>
 void trace_closest(nt_scene* s, int mesh_index, const float* d_org, const float* d_dir, long long nrays, int retest,
                    int* d_facet, float* d_t, cudaStream_t st, unsigned long long* counters)
@@ -1362,6 +1483,29 @@ nt_surface surface_or_default(const nt_surface* s)
                 return *s;
         }
         return nt_surface{{1, 1, 1}, 1, 0, {0, 0, 0}};
+}
+}
+
+namespace ntrace
+{
+int report_error(int code, const std::string& message)
+{
+        g_error = message;
+        return code;
+}
+
+int render_with_scratch(nt_scene* scene, const nt_render_opts* opts, double* d_accum, int64_t sample_offset,
+                        cudaStream_t stream, void* scratch, size_t scratch_bytes, nt_stats* stats)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!opts)
+                {
+                        fail(NT_EINVAL, "opts is NULL");
+                }
+                dispatch<NoallocF>(scene->n, scene, *opts, d_accum, (long long)sample_offset, stream ? stream : scene->stream,
+                                   scratch, scratch_bytes, stats);
+        });
 }
 }
 
