@@ -1194,6 +1194,267 @@ __device__ bool scene_visible(const DevScene<N>& S, const Ray<N>& r, float dist,
 }
 
 // ------------------------------------------------------------------------------------------------
+// Resumable tree walk for scenes with exactly one mesh.
+//
+// The same walk as mesh_closest, cut at leaf granularity: each call of walk_step visits one leaf
+// (descent, leaf facets, exit) and says whether the walk has ended.  A lane whose walk ends takes the
+// next ray at once while the other lanes of its warp continue theirs, so warps stay full even though
+// rays visit very different numbers of leaves (the per-ray loop leaves most lanes idle).  The
+// decisions around the walk are those of ray_intersection (ray_intersection.h:26-105) and
+// light_source_is_visible (painter.cpp:142-186) specialised to one mesh plus non-mesh objects, whose
+// precise distance equals their approximate one.
+
+template <int N>
+struct Walk
+{
+        Ray<N> ray;
+        float cur[N];
+        float probe[N];
+        float travelled;
+        float root_t;
+        float tmax;
+        float ao;
+        int steps;
+        bool first;
+        PathCache pc;
+};
+
+enum WalkStatus : int
+{
+        W_RUNNING = 0,
+        W_HIT = 1,
+        W_MISS = 2
+};
+
+template <int N>
+__device__ __forceinline__ void walk_begin(Walk<N>& w, const Ray<N>& ray, float root_t, float tmax)
+{
+        w.ray = ray;
+        w.ao = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+        {
+                w.ao = fmaxf(w.ao, fabsf(ray.org[i]));
+                w.cur[i] = ray.org[i];
+                w.probe[i] = ray.org[i];
+        }
+        w.travelled = 0;
+        w.root_t = root_t;
+        w.tmax = tmax;
+        w.steps = 0;
+        w.first = true;
+        w.pc.depth = -1;
+        w.pc.bits = 0;
+}
+
+// One leaf of SpatialSubdivisionTree::trace_ray (tree.h:534-590) for mesh M.
+template <int N>
+__device__ __forceinline__ int walk_step(const MeshDev<N>& M, Walk<N>& w, int retest, float* t_out, int* facet_out,
+                                         WalkStats* ws)
+{
+        if (++w.steps > 16384)
+        {
+                ws->error |= ERR_WALK_LIMIT;
+                return W_MISS;
+        }
+        Leaf<N> lf;
+        int2 nd;
+        if (find_leaf_cached<N>(M, w.probe, w.pc, &lf, &nd, &ws->descent))
+        {
+                ++ws->box_steps;
+                const float* sz = M.size[lf.level];
+                if (w.travelled > w.tmax * 1.00001f + 1e-6f)
+                {
+                        return W_MISS;
+                }
+                if (nd.y > 0)
+                {
+                        Ray64Source<N> src{nullptr, nullptr, 0};
+                        float t;
+                        int f = leaf_closest<N>(M, nd, w.ray, w.ao, src, retest, &t, ws);
+                        if (f >= 0)
+                        {
+                                float pt[N];
+                                ray_point<N>(w.ray, t, pt);
+                                bool inside = true;
+#pragma unroll
+                                for (int i = 0; i < N; ++i)
+                                {
+                                        float d1 = lf.org[i] + sz[i];
+                                        if (!(pt[i] <= d1) || !(-pt[i] <= -lf.org[i]))
+                                        {
+                                                inside = false;
+                                        }
+                                }
+                                if (inside)
+                                {
+                                        *t_out = t;
+                                        *facet_out = f;
+                                        return W_HIT;
+                                }
+                        }
+                }
+                float first_t, second_t;
+                if (!box_slabs<N>(lf.org, sz, w.cur, w.ray.dir, &first_t, &second_t))
+                {
+                        return W_MISS;
+                }
+                float ip[N], d1[N];
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        ip[i] = w.cur[i] + w.ray.dir[i] * second_t;
+                        d1[i] = lf.org[i] + sz[i];
+                }
+                int ax;
+                float sg;
+                box_normal_axis<N>(lf.org, d1, ip, &ax, &sg);
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        w.cur[i] = ip[i];
+                        w.probe[i] = (i == ax) ? ip[i] + M.dist * sg : ip[i] + M.dist * 0.0f;
+                }
+                w.travelled += second_t;
+        }
+        else
+        {
+                if (!w.first)
+                {
+                        return W_MISS;
+                }
+                float ip[N];
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        ip[i] = w.cur[i] + w.ray.dir[i] * w.root_t;
+                }
+                int ax;
+                float sg;
+                box_normal_axis<N>(M.root_org, M.root_d1, ip, &ax, &sg);
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        w.cur[i] = ip[i];
+                        w.probe[i] = (i == ax) ? ip[i] - M.dist * sg : ip[i] - M.dist * 0.0f;
+                }
+                w.travelled = w.root_t;
+        }
+        w.first = false;
+        return W_RUNNING;
+}
+
+// What ray_intersection decides around the one mesh: the objects' approximate distances in stable
+// order; the walk is needed unless a non-mesh object is strictly nearer than the mesh's root box
+// (then the loop breaks before the mesh).  pre: the choice made before the mesh entry; post: the
+// nearest non-mesh entry after it, compared with the walk's result.
+struct ClosestPlan
+{
+        int mesh_obj;        // object index of the mesh
+        float mesh_t;        // its approximate distance (root box)
+        bool walk;
+        float pre_t;         // FLT_MAX: none
+        int pre_obj;
+        float post_t;        // FLT_MAX: none
+        int post_obj;
+};
+
+template <int N>
+__device__ __forceinline__ void closest_plan(const DevScene<N>& S, const Ray<N>& r, ClosestPlan* p)
+{
+        p->mesh_obj = -1;
+        p->walk = false;
+        p->pre_t = FLT_MAX;
+        p->pre_obj = -1;
+        p->post_t = FLT_MAX;
+        p->post_obj = -1;
+        float a_m = FLT_MAX;
+        bool mesh_hit = false;
+        for (int o = 0; o < S.nobj; ++o)
+        {
+                if (S.obj[o].kind == OBJ_MESH)
+                {
+                        p->mesh_obj = o;
+                        mesh_hit = obj_approx<N>(S, o, r, &a_m);
+                        break;
+                }
+        }
+        // entries before the mesh in the stable ascending order: a < a_m, or a == a_m with a smaller
+        // object index; after it: a > a_m, or a == a_m with a larger index
+        float best_pre = FLT_MAX, best_post = FLT_MAX;
+        int pre_obj = -1, post_obj = -1;
+        for (int o = 0; o < S.nobj; ++o)
+        {
+                if (o == p->mesh_obj)
+                {
+                        continue;
+                }
+                float a;
+                if (!obj_approx<N>(S, o, r, &a))
+                {
+                        continue;
+                }
+                bool before = !mesh_hit || a < a_m || (a == a_m && o < p->mesh_obj);
+                if (before)
+                {
+                        if (a < best_pre)
+                        {
+                                best_pre = a;
+                                pre_obj = o;
+                        }
+                }
+                else if (a < best_post)
+                {
+                        best_post = a;
+                        post_obj = o;
+                }
+        }
+        p->mesh_t = a_m;
+        if (!mesh_hit)
+        {
+                p->pre_t = best_pre;
+                p->pre_obj = pre_obj;
+                return;
+        }
+        if (pre_obj >= 0 && best_pre < a_m)
+        {
+                // the loop takes the nearest entry and breaks at the mesh
+                p->pre_t = best_pre;
+                p->pre_obj = pre_obj;
+                return;
+        }
+        p->walk = true;
+        p->pre_t = best_pre;  // a tie at a_m, or none
+        p->pre_obj = pre_obj;
+        p->post_t = best_post;
+        p->post_obj = post_obj;
+}
+
+// The loop's choice once the walk has given (hit, d) for the mesh.
+__device__ __forceinline__ void closest_finish(const ClosestPlan& p, bool hit, float d, int facet, float* t_out,
+                                               int* obj_out, int* facet_out)
+{
+        float mn = p.pre_t;
+        int obj = p.pre_obj;
+        int fct = -1;
+        if (hit && d < mn)
+        {
+                mn = d;
+                obj = p.mesh_obj;
+                fct = facet;
+        }
+        if (p.post_obj >= 0 && !(mn < p.post_t) && p.post_t < mn)
+        {
+                mn = p.post_t;
+                obj = p.post_obj;
+                fct = -1;
+        }
+        *t_out = mn;
+        *obj_out = obj;
+        *facet_out = fct;
+}
+
+// ------------------------------------------------------------------------------------------------
 // Sampling (sphere.h:87-116, complement.h:71-200)
 
 template <int N>

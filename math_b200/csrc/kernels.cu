@@ -13,6 +13,8 @@ namespace
 constexpr int BLOCK = 256;
 // resident blocks per SM asked of the tree-walk kernels (caps their registers at 65536 / (3 x 256))
 constexpr int WALK_MIN_BLOCKS = 3;
+// fill rounds per iteration of the lane-refill walks
+constexpr int FILL_ROUNDS = 8;
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -535,6 +537,222 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_consta
         flush_stats<true>(counters, ws, 0, rays);
 }
 
+// Lane-level refill: every lane that has no ray takes the next one from the queue (one atomic per
+// warp for all of them), and every lane with a ray advances it by one tree leaf.  Returns, for each
+// lane, the queue index it took (-1: none); the warp knows the queue is drained when `exhausted`.
+__device__ __forceinline__ long long lane_refill(bool idle, unsigned long long* work, long long count, bool* exhausted)
+{
+        const unsigned full = 0xffffffffu;
+        unsigned need = __ballot_sync(full, idle);
+        if (!need || *exhausted)
+        {
+                return -1;
+        }
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(need) - 1;
+        const int cnt = __popc(need);
+        long long base = 0;
+        if (lane == leader)
+        {
+                base = (long long)atomicAdd(work, (unsigned long long)cnt);
+        }
+        base = __shfl_sync(full, base, leader);
+        if (base + cnt >= count)
+        {
+                *exhausted = true;
+        }
+        if (!idle)
+        {
+                return -1;
+        }
+        long long j = base + __popc(need & lanemask_lt());
+        return j < count ? j : -1;
+}
+
+// Extension rays of a scene with one mesh: closest_plan at fetch, then one leaf per iteration.
+template <int N>
+__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
+        k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, long long count,
+                        unsigned long long* counters)
+{
+        const MeshDev<N>& M = S.mesh[0];
+        WalkStats ws{0, 0, 0, 0, 0};
+        long long rays = 0;
+        long long i = -1;
+        bool exhausted = false;
+        Walk<N> w;
+        ClosestPlan plan;
+        while (true)
+        {
+                // fill: rays that need no walk are finished here, so keep taking rays (a bounded number
+                // of rounds) until every lane holds one that does
+                for (int round = 0; round < FILL_ROUNDS; ++round)
+                {
+                        long long j = lane_refill(i < 0, counters + C_WORK_EXT, count, &exhausted);
+                        if (j >= 0)
+                        {
+                                ++rays;
+                                Ray<N> r;
+#pragma unroll
+                                for (int k = 0; k < N; ++k)
+                                {
+                                        r.org[k] = A.at(k, j);
+                                        r.dir[k] = A.at(N + k, j);
+                                }
+                                closest_plan<N>(S, r, &plan);
+                                if (plan.walk)
+                                {
+                                        walk_begin<N>(w, r, plan.mesh_t, FLT_MAX);
+                                        i = j;
+                                }
+                                else if (plan.pre_obj >= 0)
+                                {
+                                        H.t[j] = plan.pre_t;
+                                        H.obj[j] = plan.pre_obj;
+                                        H.facet[j] = -1;
+                                }
+                                else
+                                {
+                                        H.obj[j] = -1;
+                                }
+                        }
+                        if (exhausted || !__any_sync(0xffffffffu, i < 0))
+                        {
+                                break;
+                        }
+                }
+                if (!__any_sync(0xffffffffu, i >= 0))
+                {
+                        if (exhausted)
+                        {
+                                break;
+                        }
+                        continue;
+                }
+                if (i >= 0)
+                {
+                        float t = 0;
+                        int f = -1;
+                        int status = walk_step<N>(M, w, S.retest, &t, &f, &ws);
+                        if (status != W_RUNNING)
+                        {
+                                float tt;
+                                int obj, fct;
+                                closest_finish(plan, status == W_HIT, t, f, &tt, &obj, &fct);
+                                if (obj >= 0)
+                                {
+                                        H.t[i] = tt;
+                                        H.obj[i] = obj;
+                                        H.facet[i] = fct;
+                                }
+                                else
+                                {
+                                        H.obj[i] = -1;
+                                }
+                                i = -1;
+                        }
+                }
+        }
+        flush_stats<false>(counters, ws, rays, 0);
+}
+
+// Shadow rays of a scene with one mesh: a non-mesh object nearer than the light occludes at once;
+// otherwise the mesh is walked (up to the light's distance) when its root box starts before the light.
+template <int N>
+__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
+        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, long long count,
+                        unsigned long long* counters)
+{
+        const MeshDev<N>& M = S.mesh[0];
+        WalkStats ws{0, 0, 0, 0, 0};
+        long long rays = 0;
+        long long i = -1;
+        bool exhausted = false;
+        Walk<N> w;
+        float dist = 0;
+        while (true)
+        {
+                for (int round = 0; round < FILL_ROUNDS; ++round)
+                {
+                        long long j = lane_refill(i < 0, counters + C_WORK_SH, count, &exhausted);
+                        if (j >= 0)
+                        {
+                                ++rays;
+                                Ray<N> r;
+#pragma unroll
+                                for (int k = 0; k < N; ++k)
+                                {
+                                        r.org[k] = SQ.at(k, j);
+                                        r.dir[k] = SQ.at(N + k, j);
+                                }
+                                float dj = SQ.at(2 * N, j);
+                                bool occluded = false;
+                                bool walk = false;
+                                float a_m = 0;
+                                for (int o = 0; o < S.nobj; ++o)
+                                {
+                                        float a;
+                                        if (!obj_approx<N>(S, o, r, &a) || !(a < dj))
+                                        {
+                                                continue;
+                                        }
+                                        if (S.obj[o].kind == OBJ_MESH)
+                                        {
+                                                walk = true;
+                                                a_m = a;
+                                        }
+                                        else
+                                        {
+                                                occluded = true;
+                                        }
+                                }
+                                if (!occluded)
+                                {
+                                        if (walk)
+                                        {
+                                                walk_begin<N>(w, r, a_m, dj);
+                                                dist = dj;
+                                                i = j;
+                                        }
+                                        else
+                                        {
+                                                accumulate(accum, SQ.pix[j], SQ.at(2 * N + 1, j), SQ.at(2 * N + 2, j),
+                                                           SQ.at(2 * N + 3, j));
+                                        }
+                                }
+                        }
+                        if (exhausted || !__any_sync(0xffffffffu, i < 0))
+                        {
+                                break;
+                        }
+                }
+                if (!__any_sync(0xffffffffu, i >= 0))
+                {
+                        if (exhausted)
+                        {
+                                break;
+                        }
+                        continue;
+                }
+                if (i >= 0)
+                {
+                        float t = 0;
+                        int f = -1;
+                        int status = walk_step<N>(M, w, S.retest, &t, &f, &ws);
+                        if (status != W_RUNNING)
+                        {
+                                if (!(status == W_HIT && t < dist))
+                                {
+                                        accumulate(accum, SQ.pix[i], SQ.at(2 * N + 1, i), SQ.at(2 * N + 2, i),
+                                                   SQ.at(2 * N + 3, i));
+                                }
+                                i = -1;
+                        }
+                }
+        }
+        flush_stats<true>(counters, ws, 0, rays);
+}
+
 template <int N>
 long long grid_for(long long count)
 {
@@ -611,6 +829,10 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
         const long long path_base = P.path_begin;
         static const long long extend_blocks = resident_blocks(k_extend<N>);
         static const long long shadow_blocks = resident_blocks(k_shadow<N>);
+        static const long long extend_refill_blocks = resident_blocks(k_extend_refill<N>);
+        static const long long shadow_refill_blocks = resident_blocks(k_shadow_refill<N>);
+        // scenes with exactly one mesh use the lane-refill walk kernels
+        const bool one_mesh = S.nmesh == 1;
         for (int iter = 0; active > 0 || next < total_paths; ++iter)
         {
                 if (stop && *stop)
@@ -642,8 +864,16 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                         cudaEventRecord(ev[1], st);
                 }
                 cudaMemsetAsync(counters + C_WORK_EXT, 0, 2 * sizeof(unsigned long long), st);
-                k_extend<N><<<(unsigned)std::min(extend_blocks, grid_for<N>(active)), BLOCK, 0, st>>>(S, A, H, active,
-                                                                                                      counters);
+                if (one_mesh)
+                {
+                        k_extend_refill<N><<<(unsigned)std::min(extend_refill_blocks, grid_for<N>(active)), BLOCK, 0, st>>>(
+                                S, A, H, active, counters);
+                }
+                else
+                {
+                        k_extend<N><<<(unsigned)std::min(extend_blocks, grid_for<N>(active)), BLOCK, 0, st>>>(S, A, H, active,
+                                                                                                              counters);
+                }
                 if (timing)
                 {
                         cudaEventRecord(ev[2], st);
@@ -663,7 +893,12 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                 }
                 long long survivors = (long long)host_counters[C_ACTIVE_OUT];
                 long long shadows = (long long)host_counters[C_SHADOW];
-                if (shadows > 0)
+                if (shadows > 0 && one_mesh)
+                {
+                        k_shadow_refill<N><<<(unsigned)std::min(shadow_refill_blocks, grid_for<N>(shadows)), BLOCK, 0, st>>>(
+                                S, SQ, accum, shadows, counters);
+                }
+                else if (shadows > 0)
                 {
                         k_shadow<N><<<(unsigned)std::min(shadow_blocks, grid_for<N>(shadows)), BLOCK, 0, st>>>(
                                 S, SQ, accum, shadows, counters);

@@ -1188,9 +1188,11 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st)
         {
                 fail(NT_EINVAL, "sample count overflow");
         }
-        long long Q = o.pool_paths > 0 ? o.pool_paths : (1ll << 20);
-        Q = std::max<long long>(256, std::min(Q, total));
         const int lights = (int)s->lights.size();
+        // default pool: 4 Mi paths (fewer wavefront iterations, so less per-launch tail), at most 1 GiB
+        const long long per_path = (long long)(Wavefront<N>::bytes_for(1, lights) - Wavefront<N>::bytes_for(0, lights));
+        long long Q = o.pool_paths > 0 ? o.pool_paths : std::min<long long>(1ll << 22, (1ll << 30) / per_path);
+        Q = std::max<long long>(256, std::min(Q, total));
         if (Q > s->pool_paths || lights > s->pool_lights)
         {
                 s->pool.alloc(Wavefront<N>::bytes_for(Q, lights));
