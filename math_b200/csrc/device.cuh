@@ -260,14 +260,31 @@ __device__ __forceinline__ void box_normal_axis(const float* org_box, const floa
 template <int N>
 struct Leaf
 {
-        int node;
+        int node;  // -1: no leaf contains the point
         int level;
         float org[N];
 };
 
 template <int N>
-__device__ __noinline__ bool find_leaf_dfs(const MeshDev<N>& M, const float* p, Leaf<N>* out)
+struct Point
 {
+        float v[N];
+};
+
+// Out of line and by value: the caller's walk state is not address-taken, so it stays in registers.
+template <int N>
+__device__ __noinline__ Leaf<N> find_leaf_dfs(const MeshDev<N>& M, const Point<N> pt)
+{
+        const float* p = pt.v;
+        Leaf<N> res;
+        res.node = -1;
+        res.level = 0;
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+        {
+                res.org[i] = 0;
+        }
+        Leaf<N>* out = &res;
         struct Frame
         {
                 int node;
@@ -295,7 +312,7 @@ __device__ __noinline__ bool find_leaf_dfs(const MeshDev<N>& M, const float* p, 
                         {
                                 out->org[i] = f.org[i];
                         }
-                        return true;
+                        return res;
                 }
                 bool pushed = false;
                 while (f.next < (1 << N) && top < MAX_LEVELS)
@@ -332,8 +349,12 @@ __device__ __noinline__ bool find_leaf_dfs(const MeshDev<N>& M, const float* p, 
                         --top;
                 }
         }
-        return false;
+        return res;
 }
+
+// Threads per block of every kernel that walks a tree: the path caches' per-level slots are laid
+// out in shared memory with this stride.
+constexpr int WALK_BLOCK = 256;
 
 // The root-to-leaf path of the previous point location of the same walk.  Consecutive leaves of a
 // walk share most of their ancestors; the child chosen at each level depends only on the point and
@@ -344,14 +365,28 @@ struct PathCache
         int depth;                 // level of the cached leaf; -1: empty
         unsigned long long bits;   // child index chosen at each level, 6 bits per level
         int2 leaf;                 // the cached leaf's record
-        int leaf_node;
-        int fc[MAX_LEVELS];        // first child of the internal node at each level of the path
+        // the first child of the internal node at each level of the path is kept in shared memory
+        // (path_cache_slots)
+
+        __device__ __forceinline__ void reset()
+        {
+                depth = -1;
+                bits = 0;
+        }
 };
+
+// This thread's column of the block's path-cache slots (MAX_LEVELS x WALK_BLOCK ints).
+__device__ __forceinline__ int* path_cache_slots()
+{
+        __shared__ int s_fc[MAX_LEVELS * WALK_BLOCK];
+        return s_fc + threadIdx.x;
+}
 
 template <int N>
 __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const float* p, PathCache& pc, Leaf<N>* out,
-                                                 int2* leaf_rec, long long* descent)
+                                                 int2* leaf_rec, unsigned* descent)
 {
+        int* const fc = path_cache_slots();
 #pragma unroll
         for (int i = 0; i < N; ++i)
         {
@@ -374,7 +409,7 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                 int2 nd;
                 if (same)
                 {
-                        nd = (lvl == pc.depth) ? pc.leaf : make_int2(pc.fc[lvl], -1);
+                        nd = (lvl == pc.depth) ? pc.leaf : make_int2(fc[lvl * WALK_BLOCK], -1);
                 }
                 else
                 {
@@ -393,12 +428,11 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                         *leaf_rec = nd;
                         pc.depth = lvl;
                         pc.leaf = nd;
-                        pc.leaf_node = node;
                         return true;
                 }
                 if (!same)
                 {
-                        pc.fc[lvl] = nd.x;
+                        fc[lvl * WALK_BLOCK] = nd.x;
                 }
                 int child = 0;
                 bool fail = false;
@@ -428,12 +462,18 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                         pc.depth = -1;
                         if (ambiguous)
                         {
-                                bool found = find_leaf_dfs<N>(M, p, out);
-                                if (found)
+                                Point<N> pt;
+#pragma unroll
+                                for (int i = 0; i < N; ++i)
+                                {
+                                        pt.v[i] = p[i];
+                                }
+                                *out = find_leaf_dfs<N>(M, pt);
+                                if (out->node >= 0)
                                 {
                                         *leaf_rec = __ldg(&M.nodes[out->node]);
+                                        return true;
                                 }
-                                return found;
                         }
                         return false;
                 }
@@ -446,72 +486,6 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                 node = nd.x + child;
         }
         pc.depth = -1;
-        return false;
-}
-
-template <int N>
-__device__ __forceinline__ bool find_leaf(const MeshDev<N>& M, const float* p, Leaf<N>* out, long long* descent)
-{
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-        {
-                if (!(p[i] <= M.root_d1[i]) || !(-p[i] <= -M.root_org[i]))
-                {
-                        return false;
-                }
-        }
-        float o[N];
-#pragma unroll
-        for (int i = 0; i < N; ++i)
-        {
-                o[i] = M.root_org[i];
-        }
-        int node = 0;
-        bool ambiguous = false;
-        for (int lvl = 0; lvl < MAX_LEVELS; ++lvl)
-        {
-                int2 nd = __ldg(&M.nodes[node]);
-                ++*descent;
-                if (nd.y >= 0)
-                {
-                        out->node = node;
-                        out->level = lvl;
-#pragma unroll
-                        for (int i = 0; i < N; ++i)
-                        {
-                                out->org[i] = o[i];
-                        }
-                        return true;
-                }
-                int child = 0;
-                bool fail = false;
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                {
-                        float h = M.size[lvl + 1][i];
-                        float mid = o[i] + h;
-                        bool lo_ok = p[i] <= mid;
-                        bool hi_ok = (-p[i] <= -mid) && (p[i] <= mid + h);
-                        if (lo_ok)
-                        {
-                                ambiguous |= hi_ok;
-                        }
-                        else if (hi_ok)
-                        {
-                                child |= 1 << i;
-                                o[i] = mid;
-                        }
-                        else
-                        {
-                                fail = true;
-                        }
-                }
-                if (fail)
-                {
-                        return ambiguous ? find_leaf_dfs<N>(M, p, out) : false;
-                }
-                node = nd.x + child;
-        }
         return false;
 }
 
@@ -554,7 +528,9 @@ __device__ __forceinline__ int facet_test32(const float4* rec, const Ray<N>& r, 
         float e_num = 8.0f * EPS * (fabsf(d0) + N * ao);
         if (as < 1e-6f)
         {
-                // grazing: the reference tests s != 0 in FP64; decide there
+                // grazing: the reference tests s != 0 in FP64; decide there (without the re-test the
+                // FP32 distance stands, and a ray parallel to the plane gets none)
+                *t_out = (as > 0) ? __fdiv_rn(num, s) : -1.0f;
                 return (as == 0 && fabsf(num) > e_num) ? T_MISS : T_UNSURE;
         }
         float t = __fdiv_rn(num, s);
@@ -722,23 +698,26 @@ struct Ray64Source
         }
 };
 
+// Per-thread work counters of one launch (flushed to the 64-bit device counters at the end).
 struct WalkStats
 {
-        long long facet_tests;
-        long long box_steps;
-        long long retests;
-        long long descent;
+        unsigned facet_tests;
+        unsigned box_steps;
+        unsigned retests;
+        unsigned descent;
         int error;
 };
 
 // FP64 re-test of one facet, kept out of line so that its double-precision state does not occupy
-// registers of the hot FP32 walk.
+// registers of the hot FP32 walk; arguments by value so that the caller's ray is not address-taken.
+// Returns the FP64 distance, or -1 when the facet is missed.
 template <int N>
-__device__ __noinline__ bool retest_facet(const double* rec, const Ray<N>& ray, const Ray64Source<N>& src, double* t)
+__device__ __noinline__ double retest_facet(const double* rec, const Ray<N> ray, const Ray64Source<N> src)
 {
         Ray64<N> r64;
         src.get(ray, &r64);
-        return facet_test64<N>(rec, r64, t);
+        double t;
+        return facet_test64<N>(rec, r64, &t) ? t : -1.0;
 }
 
 // Closest facet of one leaf (ray_intersection over indices, ray_intersection.h:134-159: strict <
@@ -777,7 +756,8 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
                         else
                         {
                                 ++ws->retests;
-                                if (!retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, src, &t64))
+                                t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, src);
+                                if (!(t64 > 0))
                                 {
                                         continue;
                                 }
@@ -793,7 +773,8 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
                         if (!is64)
                         {
                                 ++ws->retests;
-                                if (!retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, src, &t64))
+                                t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, src);
+                                if (!(t64 > 0))
                                 {
                                         continue;
                                 }
@@ -802,8 +783,8 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
                         if (!b64)
                         {
                                 ++ws->retests;
-                                double tb;
-                                if (retest_facet<N>(M.rec64 + (size_t)best * Rec64<N>::DOUBLES, ray, src, &tb))
+                                double tb = retest_facet<N>(M.rec64 + (size_t)best * Rec64<N>::DOUBLES, ray, src);
+                                if (tb > 0)
                                 {
                                         bt64 = tb;
                                         b64 = true;
@@ -860,8 +841,7 @@ __device__ bool mesh_closest(const MeshDev<N>& M, const Ray<N>& ray, float root_
         float travelled = 0;
         bool first = true;
         PathCache pc;
-        pc.depth = -1;
-        pc.bits = 0;
+        pc.reset();
         // a ray crosses at most (boxes per axis) x N leaves of a 2^N-tree at most 2^9 boxes wide;
         // the bound leaves ample margin and turns a walk that does not advance into an error flag
         for (int step = 0; step < 16384; ++step)
@@ -1196,27 +1176,41 @@ __device__ bool scene_visible(const DevScene<N>& S, const Ray<N>& r, float dist,
 // ------------------------------------------------------------------------------------------------
 // Resumable tree walk for scenes with exactly one mesh.
 //
-// The same walk as mesh_closest, cut at leaf granularity: each call of walk_step visits one leaf
-// (descent, leaf facets, exit) and says whether the walk has ended.  A lane whose walk ends takes the
-// next ray at once while the other lanes of its warp continue theirs, so warps stay full even though
-// rays visit very different numbers of leaves (the per-ray loop leaves most lanes idle).  The
-// decisions around the walk are those of ray_intersection (ray_intersection.h:26-105) and
+// The same walk as mesh_closest, cut at leaf granularity: each call of walk_step_warp visits one
+// leaf (descent, leaf facets, exit) and says whether the walk has ended.  A lane whose walk ends
+// takes the next ray at once while the other lanes of its warp continue theirs, so warps stay full
+// even though rays visit very different numbers of leaves (the per-ray loop leaves most lanes idle).
+// The decisions around the walk are those of ray_intersection (ray_intersection.h:26-105) and
 // light_source_is_visible (painter.cpp:142-186) specialised to one mesh plus non-mesh objects, whose
 // precise distance equals their approximate one.
+//
+// The state is kept small (it stays in registers across the pooled facet tests): the probe point is
+// the current point nudged along one axis, stored as that axis and direction; the root-box entry
+// distance sits in `travelled` until the first step.
 
 template <int N>
 struct Walk
 {
         Ray<N> ray;
         float cur[N];
-        float probe[N];
         float travelled;
-        float root_t;
         float tmax;
         float ao;
         int steps;
-        bool first;
+        int nudge;      // 0: the probe is cur; +-(axis + 1): cur nudged by +-dist along axis
+        long long raw;  // index of the caller's raw ray (fixed-ray-set query), for the FP64 re-test
         PathCache pc;
+
+        __device__ __forceinline__ void probe(float dist, float* p) const
+        {
+                const int ax = (nudge > 0 ? nudge : -nudge) - 1;
+                const float s = nudge > 0 ? dist : -dist;
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        p[i] = (i == ax) ? cur[i] + s : cur[i];
+                }
+        }
 };
 
 enum WalkStatus : int
@@ -1236,62 +1230,285 @@ __device__ __forceinline__ void walk_begin(Walk<N>& w, const Ray<N>& ray, float 
         {
                 w.ao = fmaxf(w.ao, fabsf(ray.org[i]));
                 w.cur[i] = ray.org[i];
-                w.probe[i] = ray.org[i];
         }
-        w.travelled = 0;
-        w.root_t = root_t;
+        w.travelled = root_t;
         w.tmax = tmax;
         w.steps = 0;
-        w.first = true;
-        w.pc.depth = -1;
-        w.pc.bits = 0;
+        w.nudge = 0;
+        w.raw = 0;
+        // the path cache describes a root-to-leaf path of the tree, not the ray: it stays valid
+        // from one ray of the lane to the next (neighbouring rays share their upper levels), so it
+        // is reset once per lane (w.pc.reset()) and not here
 }
 
-// One leaf of SpatialSubdivisionTree::trace_ray (tree.h:534-590) for mesh M.
-template <int N>
-__device__ __forceinline__ int walk_step(const MeshDev<N>& M, Walk<N>& w, int retest, float* t_out, int* facet_out,
-                                         WalkStats* ws)
+// ------------------------------------------------------------------------------------------------
+// Warp-cooperative leaf step.
+//
+// The leaves that the 32 lanes of a warp stand in hold different numbers of facets (0 to a few
+// dozen), so a per-lane loop over them leaves most lanes idle.  Here the warp pools its facet tests:
+// the lanes' facet lists are laid end to end (warp prefix sum of the counts) and every lane tests
+// every 32nd entry of the pooled list against the owning lane's ray, fetched by shuffle.  Each
+// outcome (FP32 hit, or hit after the FP64 re-test) goes to a per-warp shared-memory slot; the owner
+// then reads its own slots in leaf-list order and makes the same sequential choice as leaf_closest
+// (strict < in list order, near-ties settled in FP64), so the result is the per-lane loop's.
+
+constexpr int POOL_SLOTS = 128;  // pooled tests per warp and round
+
+struct PoolSlot
 {
-        if (++w.steps > 16384)
-        {
-                ws->error |= ERR_WALK_LIMIT;
-                return W_MISS;
-        }
-        Leaf<N> lf;
-        int2 nd;
-        if (find_leaf_cached<N>(M, w.probe, w.pc, &lf, &nd, &ws->descent))
-        {
-                ++ws->box_steps;
-                const float* sz = M.size[lf.level];
-                if (w.travelled > w.tmax * 1.00001f + 1e-6f)
-                {
-                        return W_MISS;
-                }
-                if (nd.y > 0)
-                {
-                        Ray64Source<N> src{nullptr, nullptr, 0};
-                        float t;
-                        int f = leaf_closest<N>(M, nd, w.ray, w.ao, src, retest, &t, ws);
-                        if (f >= 0)
-                        {
-                                float pt[N];
-                                ray_point<N>(w.ray, t, pt);
-                                bool inside = true;
+        float t;      // FP32 distance (the rounded FP64 one after a re-test)
+        int facet;    // -1: missed
+        double t64;   // FP64 distance when re-tested; -1 otherwise
+};
+
+__device__ __forceinline__ PoolSlot* warp_pool()
+{
+        __shared__ PoolSlot s_pool[(WALK_BLOCK / 32) * POOL_SLOTS];
+        return s_pool + (threadIdx.x >> 5) * POOL_SLOTS;
+}
+
+// Closest facet of this lane's leaf (facets leaf_idx[start .. start + cnt)); every lane of the warp
+// calls it, lanes without a leaf with cnt = 0.  raw_org/raw_dir: the caller's raw rays for the
+// FP64 re-test of the fixed-ray-set query (null when rendering: the FP32 ray is promoted).
+template <int N>
+__device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start, int cnt, const Ray<N>& ray, float ao,
+                                                 long long raw, const float* raw_org, const float* raw_dir, int retest,
+                                                 float* t_best, WalkStats* ws)
+{
+        const unsigned full = 0xffffffffu;
+        const int lane = threadIdx.x & 31;
+        int incl = cnt;
 #pragma unroll
-                                for (int i = 0; i < N; ++i)
+        for (int d = 1; d < 32; d <<= 1)
+        {
+                int v = __shfl_up_sync(full, incl, d);
+                if (lane >= d)
+                {
+                        incl += v;
+                }
+        }
+        const int total = __shfl_sync(full, incl, 31);
+        const int excl = incl - cnt;
+        int best = -1;
+        float bt = FLT_MAX;
+        double bt64 = 0;
+        bool b64 = false;
+        if (total == 0)
+        {
+                *t_best = bt;
+                return best;
+        }
+        PoolSlot* pool = warp_pool();
+        const Ray64Source<N> own_src{raw_org, raw_dir, raw};
+        for (int cb = 0; cb < total; cb += POOL_SLOTS)
+        {
+                const int ce = min(total, cb + POOL_SLOTS);
+                for (int k0 = cb; k0 < ce; k0 += 32)
+                {
+                        const int k = k0 + lane;
+                        // owner: the last lane whose list starts at or before k
+                        int o = 0;
+#pragma unroll
+                        for (int step = 16; step > 0; step >>= 1)
+                        {
+                                int v = __shfl_sync(full, excl, o + step);
+                                if (v <= k)
                                 {
-                                        float d1 = lf.org[i] + sz[i];
-                                        if (!(pt[i] <= d1) || !(-pt[i] <= -lf.org[i]))
+                                        o += step;
+                                }
+                        }
+                        const int o_start = __shfl_sync(full, start, o);
+                        const int o_excl = __shfl_sync(full, excl, o);
+                        const float o_ao = __shfl_sync(full, ao, o);
+                        Ray<N> r;
+#pragma unroll
+                        for (int i = 0; i < N; ++i)
+                        {
+                                r.org[i] = __shfl_sync(full, ray.org[i], o);
+                                r.dir[i] = __shfl_sync(full, ray.dir[i], o);
+                        }
+                        const long long o_raw = raw_org ? __shfl_sync(full, raw, o) : 0;
+                        if (k < ce)
+                        {
+                                const int f = __ldg(&M.leaf_idx[o_start + (k - o_excl)]);
+                                ++ws->facet_tests;
+                                float t = -1.0f;
+                                double t64 = -1.0;
+                                int keep = -1;
+                                int res = facet_test32<N>(M.rec32 + (size_t)f * Rec32<N>::F4, r, o_ao, &t);
+                                if (res == T_HIT)
+                                {
+                                        keep = f;
+                                }
+                                else if (res == T_UNSURE)
+                                {
+                                        if (!retest)
                                         {
-                                                inside = false;
+                                                // without the re-test an uncertain FP32 hit counts when
+                                                // its distance is positive
+                                                if (t > 0)
+                                                {
+                                                        keep = f;
+                                                }
+                                        }
+                                        else
+                                        {
+                                                ++ws->retests;
+                                                t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, r,
+                                                                      Ray64Source<N>{raw_org, raw_dir, o_raw});
+                                                if (t64 > 0)
+                                                {
+                                                        keep = f;
+                                                        t = (float)t64;
+                                                }
+                                                else
+                                                {
+                                                        t64 = -1.0;
+                                                }
                                         }
                                 }
-                                if (inside)
+                                PoolSlot& s = pool[k - cb];
+                                s.t = t;
+                                s.facet = keep;
+                                s.t64 = t64;
+                        }
+                }
+                __syncwarp();
+                // the owner's sequential choice over its slots of this round, in list order
+                const int q0 = max(excl, cb);
+                const int q1 = min(excl + cnt, ce);
+                for (int q = q0; q < q1; ++q)
+                {
+                        const PoolSlot s = pool[q - cb];
+                        if (s.facet < 0)
+                        {
+                                continue;
+                        }
+                        const int f = s.facet;
+                        float t = s.t;
+                        double t64 = s.t64;
+                        bool is64 = t64 > 0;
+                        bool closer;
+                        float tol = 1e-5f * (fabsf(t) + ao) + 1e-30f;
+                        if (retest && best >= 0 && fabsf(t - bt) <= tol)
+                        {
+                                if (!is64)
                                 {
-                                        *t_out = t;
-                                        *facet_out = f;
-                                        return W_HIT;
+                                        ++ws->retests;
+                                        t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, ray, own_src);
+                                        if (!(t64 > 0))
+                                        {
+                                                continue;
+                                        }
+                                        is64 = true;
                                 }
+                                if (!b64)
+                                {
+                                        ++ws->retests;
+                                        double tb = retest_facet<N>(M.rec64 + (size_t)best * Rec64<N>::DOUBLES, ray, own_src);
+                                        if (tb > 0)
+                                        {
+                                                bt64 = tb;
+                                                b64 = true;
+                                        }
+                                        else
+                                        {
+                                                // the incumbent fails in FP64: the newcomer wins
+                                                best = f;
+                                                bt = (float)t64;
+                                                bt64 = t64;
+                                                b64 = true;
+                                                continue;
+                                        }
+                                }
+                                closer = t64 < bt64;
+                        }
+                        else
+                        {
+                                closer = t < bt;
+                        }
+                        if (closer)
+                        {
+                                best = f;
+                                bt = t;
+                                bt64 = t64;
+                                b64 = is64;
+                        }
+                }
+                __syncwarp();
+        }
+        *t_best = bt;
+        return best;
+}
+
+// walk_step with the leaf's facets tested by leaf_closest_warp.  Every lane of the warp calls it
+// (active = false for lanes without a walk, whose result is ignored).
+template <int N>
+__device__ __forceinline__ int walk_step_warp(const MeshDev<N>& M, Walk<N>& w, bool active, int retest,
+                                              const float* raw_org, const float* raw_dir, float* t_out, int* facet_out,
+                                              WalkStats* ws)
+{
+        int status = W_MISS;
+        bool leaf = false;
+        Leaf<N> lf;
+        int2 nd = make_int2(0, 0);
+        if (active)
+        {
+                status = W_RUNNING;
+                float probe[N];
+                w.probe(M.dist, probe);
+                if (++w.steps > 16384)
+                {
+                        ws->error |= ERR_WALK_LIMIT;
+                        status = W_MISS;
+                }
+                else if (find_leaf_cached<N>(M, probe, w.pc, &lf, &nd, &ws->descent))
+                {
+                        ++ws->box_steps;
+                        if (w.steps == 1)
+                        {
+                                // the origin is inside the tree: nothing travelled yet
+                                w.travelled = 0;
+                        }
+                        if (w.travelled > w.tmax * 1.00001f + 1e-6f)
+                        {
+                                status = W_MISS;
+                        }
+                        else
+                        {
+                                leaf = true;
+                        }
+                }
+        }
+        const int cnt = (leaf && nd.y > 0) ? nd.y : 0;
+        float t = FLT_MAX;
+        const int f = leaf_closest_warp<N>(M, nd.x, cnt, w.ray, w.ao, w.raw, raw_org, raw_dir, retest, &t, ws);
+        if (status != W_RUNNING)
+        {
+                return status;
+        }
+        if (leaf)
+        {
+                const float* sz = M.size[lf.level];
+                if (f >= 0)
+                {
+                        float pt[N];
+                        ray_point<N>(w.ray, t, pt);
+                        bool inside = true;
+#pragma unroll
+                        for (int i = 0; i < N; ++i)
+                        {
+                                float d1 = lf.org[i] + sz[i];
+                                if (!(pt[i] <= d1) || !(-pt[i] <= -lf.org[i]))
+                                {
+                                        inside = false;
+                                }
+                        }
+                        if (inside)
+                        {
+                                *t_out = t;
+                                *facet_out = f;
+                                return W_HIT;
                         }
                 }
                 float first_t, second_t;
@@ -1313,21 +1530,24 @@ __device__ __forceinline__ int walk_step(const MeshDev<N>& M, Walk<N>& w, int re
                 for (int i = 0; i < N; ++i)
                 {
                         w.cur[i] = ip[i];
-                        w.probe[i] = (i == ax) ? ip[i] + M.dist * sg : ip[i] + M.dist * 0.0f;
                 }
+                // next probe: ip + dist * sg along the exit face's axis
+                w.nudge = sg > 0 ? ax + 1 : -(ax + 1);
                 w.travelled += second_t;
         }
         else
         {
-                if (!w.first)
+                if (w.steps != 1)
                 {
                         return W_MISS;
                 }
+                // outside the tree at the start: enter through the root box (travelled holds the
+                // entry distance)
                 float ip[N];
 #pragma unroll
                 for (int i = 0; i < N; ++i)
                 {
-                        ip[i] = w.cur[i] + w.ray.dir[i] * w.root_t;
+                        ip[i] = w.cur[i] + w.ray.dir[i] * w.travelled;
                 }
                 int ax;
                 float sg;
@@ -1336,11 +1556,10 @@ __device__ __forceinline__ int walk_step(const MeshDev<N>& M, Walk<N>& w, int re
                 for (int i = 0; i < N; ++i)
                 {
                         w.cur[i] = ip[i];
-                        w.probe[i] = (i == ax) ? ip[i] - M.dist * sg : ip[i] - M.dist * 0.0f;
                 }
-                w.travelled = w.root_t;
+                // next probe: ip - dist * sg along the entry face's axis
+                w.nudge = sg > 0 ? -(ax + 1) : ax + 1;
         }
-        w.first = false;
         return W_RUNNING;
 }
 

@@ -11,10 +11,18 @@ namespace ntrace
 namespace
 {
 constexpr int BLOCK = 256;
-// resident blocks per SM asked of the tree-walk kernels (caps their registers at 65536 / (3 x 256))
-constexpr int WALK_MIN_BLOCKS = 3;
+static_assert(BLOCK == WALK_BLOCK, "path-cache slots are laid out for the walk kernels' block size");
+// resident blocks per SM asked of the tree-walk kernels (caps their registers at 65536 / (2 x 256):
+// 2 blocks without spills measured faster than 3 or 4 with them)
+#ifndef NT_WALK_MIN_BLOCKS
+#define NT_WALK_MIN_BLOCKS 2
+#endif
+constexpr int WALK_MIN_BLOCKS = NT_WALK_MIN_BLOCKS;
 // fill rounds per iteration of the lane-refill walks
-constexpr int FILL_ROUNDS = 8;
+#ifndef NT_FILL_ROUNDS
+#define NT_FILL_ROUNDS 8
+#endif
+constexpr int FILL_ROUNDS = NT_FILL_ROUNDS;
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -83,8 +91,13 @@ __global__ void __launch_bounds__(BLOCK) k_trace_closest(__grid_constant__ const
                                                          int* __restrict__ facet_out, float* __restrict__ t_out,
                                                          unsigned long long* counters)
 {
-        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
         WalkStats ws{0, 0, 0, 0, 0};
+        // one ray per lane; the warp walks until all its lanes are done (no early exit: the leaf
+        // step is warp-cooperative)
+        bool walking = false;
+        Walk<N> w;
+        w.pc.reset();
         if (i < nrays)
         {
                 float o[N], d[N];
@@ -96,32 +109,48 @@ __global__ void __launch_bounds__(BLOCK) k_trace_closest(__grid_constant__ const
                 }
                 Ray<N> r;
                 ray_set<N>(r, o, d);
-                Ray64Source<N> src{org, dir, i};
                 float first, second;
-                int f = -1;
-                float t = 0;
                 if (root_slabs<N>(M, r.org, r.dir, &first, &second))
                 {
-                        float a = (first > 0) ? first : second;
-                        if (!mesh_closest<N>(M, r, a, src, retest, FLT_MAX, &t, &f, &ws))
+                        walk_begin<N>(w, r, (first > 0) ? first : second, FLT_MAX);
+                        w.raw = i;
+                        walking = true;
+                }
+                else
+                {
+                        facet_out[i] = -1;
+                        t_out[i] = 0;
+                }
+        }
+        while (__any_sync(0xffffffffu, walking))
+        {
+                float t = 0;
+                int f = -1;
+                const int status = walk_step_warp<N>(M, w, walking, retest, org, dir, &t, &f, &ws);
+                if (walking && status != W_RUNNING)
+                {
+                        walking = false;
+                        if (status == W_HIT)
                         {
-                                f = -1;
-                                t = 0;
-                        }
-                        else if (retest)
-                        {
-                                // report the distance of the chosen facet in FP64 (rounded once)
-                                Ray64<N> r64;
-                                src.get(r, &r64);
-                                double t64;
-                                if (facet_test64<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, r64, &t64))
+                                if (retest)
                                 {
-                                        t = (float)t64;
+                                        // report the distance of the chosen facet in FP64 (rounded once)
+                                        double t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, w.ray,
+                                                                     Ray64Source<N>{org, dir, i});
+                                        if (t64 > 0)
+                                        {
+                                                t = (float)t64;
+                                        }
                                 }
+                                facet_out[i] = f;
+                                t_out[i] = t;
+                        }
+                        else
+                        {
+                                facet_out[i] = -1;
+                                t_out[i] = 0;
                         }
                 }
-                facet_out[i] = f;
-                t_out[i] = t;
         }
         flush_stats<false>(counters, ws, i < nrays ? 1 : 0, 0);
 }
@@ -581,6 +610,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         long long i = -1;
         bool exhausted = false;
         Walk<N> w;
+        w.pc.reset();
         ClosestPlan plan;
         while (true)
         {
@@ -629,12 +659,11 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                         }
                         continue;
                 }
-                if (i >= 0)
                 {
                         float t = 0;
                         int f = -1;
-                        int status = walk_step<N>(M, w, S.retest, &t, &f, &ws);
-                        if (status != W_RUNNING)
+                        int status = walk_step_warp<N>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
+                        if (i >= 0 && status != W_RUNNING)
                         {
                                 float tt;
                                 int obj, fct;
@@ -669,6 +698,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         long long i = -1;
         bool exhausted = false;
         Walk<N> w;
+        w.pc.reset();
         float dist = 0;
         while (true)
         {
@@ -734,12 +764,11 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                         }
                         continue;
                 }
-                if (i >= 0)
                 {
                         float t = 0;
                         int f = -1;
-                        int status = walk_step<N>(M, w, S.retest, &t, &f, &ws);
-                        if (status != W_RUNNING)
+                        int status = walk_step_warp<N>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
+                        if (i >= 0 && status != W_RUNNING)
                         {
                                 if (!(status == W_HIT && t < dist))
                                 {
