@@ -298,20 +298,25 @@ def main() -> None:
         dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
     e2e_value = e2e_paths * world / float(e2e_all.item())
 
-    # roofline of the dominant kernel (extension), from the timed warm-up pass
+    # roofline of the dominant walk kernel (the one with the larger device time), from the timed pass
     peaks = measured_peaks()
-    ext_bytes, ext_flops = algorithmic_work(n, timed["facet_tests"], timed["box_steps"], timed["descent_levels"])
-    sh_bytes, _ = algorithmic_work(n, timed["shadow_facet_tests"], timed["shadow_box_steps"],
-                                   timed["shadow_descent_levels"])
-    ext_launch_ms = timed["extend_ms"] / max(1, timed["extend_launches"])
-    achieved = (ext_bytes / max(1, timed["extend_launches"])) / (ext_launch_ms / 1000.0) / 1e9
+    walks = {}
+    for kind, prefix in (("extend", ""), ("shadow", "shadow_")):
+        b, f = algorithmic_work(n, timed[prefix + "facet_tests"], timed[prefix + "box_steps"],
+                                timed[prefix + "descent_levels"])
+        launches_k = max(1, timed[kind + "_launches"])
+        ms = timed[kind + "_ms"] / launches_k
+        walks[kind] = {"bytes": b / launches_k, "flops": f / launches_k, "launch_ms": ms,
+                       "achieved": (b / launches_k) / (ms / 1000.0) / 1e9 if ms > 0 else 0.0}
+    dom = max(walks, key=lambda k: timed[k + "_ms"])
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get(f"{args.config}_extend_bytes_per_launch")
+            traffic = json.loads(tf.read_text()).get(f"{args.config}_{dom}_bytes_per_launch")
         except Exception:
             traffic = None
+    achieved = walks[dom]["achieved"]
 
     result = {
         "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
@@ -322,14 +327,15 @@ def main() -> None:
                 "steps": e2e_steps},
         "gpu_launches": launches,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic, "kernel": "k_extend",
+                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+                     "kernel": "k_shadow_refill" if dom == "shadow" else "k_extend_refill",
                      "peak_source": peaks["source"],
-                     "algorithmic_bytes_per_launch": ext_bytes / max(1, timed["extend_launches"]),
-                     "algorithmic_flops_per_launch": ext_flops / max(1, timed["extend_launches"]),
-                     "launch_ms": ext_launch_ms},
+                     "algorithmic_bytes_per_launch": walks[dom]["bytes"],
+                     "algorithmic_flops_per_launch": walks[dom]["flops"],
+                     "launch_ms": walks[dom]["launch_ms"]},
         "kernels_ms_per_frame": {"raygen": timed["raygen_ms"], "extend": timed["extend_ms"], "shade": timed["shade_ms"],
                                  "shadow": timed["shadow_ms"]},
-        "shadow_algorithmic_gbs": (sh_bytes / (timed["shadow_ms"] / 1000.0) / 1e9) if timed["shadow_ms"] else None,
+        "walk_algorithmic_gbs": {k: w["achieved"] for k, w in walks.items()},
         "counters_per_frame": {k: timed[k] for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests",
                                                      "descent_levels", "shadow_facet_tests", "shadow_box_steps",
                                                      "shadow_retests", "shadow_descent_levels")},

@@ -144,7 +144,18 @@ int nt_scene_set_projector(nt_scene* scene, int kind, const float* camera_org, c
 /* PaintObjects::default_surface_properties (objects.h:222): what a ray that hits nothing returns. */
 int nt_scene_set_background(nt_scene* scene, const nt_surface* surface);
 
-/* Facet setup, 2^n-tree build and upload to the device (the work of Mesh's constructor). */
+/* Removes every light source (add the new ones before the next nt_scene_build).  No counterpart in
+ * the reference, where a PaintObjects is assembled once; here it lets one scene be relit without
+ * rebuilding its meshes' trees. */
+int nt_scene_clear_lights(nt_scene* scene);
+
+/* Replaces the surface of object `object` (objects numbered in the order they were added).  No
+ * counterpart in the reference (see nt_scene_clear_lights). */
+int nt_scene_set_object_surface(nt_scene* scene, int object, const nt_surface* surface);
+
+/* Facet setup, 2^n-tree build and upload to the device (the work of Mesh's constructor).  A rebuild
+ * after edits that leave the meshes unchanged (lights, surfaces, projector, background) reuses the
+ * meshes' facet setup, trees and device arrays. */
 int nt_scene_build(nt_scene* scene, const nt_build_opts* opts);
 
 int nt_scene_mesh_info(nt_scene* scene, int mesh_index, nt_mesh_info* info);
@@ -177,6 +188,20 @@ int nt_render_noalloc(nt_scene* scene, const nt_render_opts* opts, double* d_acc
                       void* stream, nt_stats* stats);
 
 int nt_accum_clear(nt_scene* scene);
+
+/* ---- denoiser inputs (no counterpart in the reference; see include/ntrace_denoise.h) ---- */
+
+/* First hit of every pixel-centre camera ray: the unit geometric normal turned towards the camera
+ * (pixel_count x n floats, zeros on a miss) and the hit distance (pixel_count floats, 0 on a miss),
+ * into device arrays.  stream: a cudaStream_t, NULL for the scene's stream. */
+int nt_render_aux(nt_scene* scene, float* d_normal, float* d_depth, void* stream);
+
+/* `passes` single-sample passes (sample indices sample_offset, sample_offset + 1, ...; opts gives the
+ * seed, depth and re-test, its samples_per_pixel is ignored) and, per pixel, the mean radiance and
+ * the variance of that mean (sample variance / passes; 0 for one pass), into device arrays of
+ * pixel_count x 3 floats.  Uses and clears the scene's accumulator. */
+int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int passes, int64_t sample_offset, float* d_mean,
+                      float* d_var, nt_stats* stats);
 
 /* Mean colour per pixel (pixel_count x 3 floats, x0 fastest) and the samples behind it. */
 int nt_accum_read(nt_scene* scene, float* rgb_mean, int64_t* samples_per_pixel);

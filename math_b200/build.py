@@ -82,9 +82,19 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
-    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj]):
+    denoise = CSRC / "denoise.cu"
+    denoise_obj = BUILD_DIR / "denoise.o"
+    if force or _stale(denoise_obj, [denoise] + headers + [INCLUDE / "ntrace_denoise.h"]):
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *common, "-c", str(denoise), "-o",
+               str(denoise_obj)]
+        if ptxas_info:
+            cmd.insert(1, "-Xptxas=-v")
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
+    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, denoise_obj]):
         cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj),
-               str(noalloc_obj), "-Xlinker", "--no-undefined", "-lpthread"]
+               str(noalloc_obj), str(denoise_obj), "-Xlinker", "--no-undefined", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

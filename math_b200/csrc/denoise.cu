@@ -1,0 +1,1261 @@
+// Learned kernel-predicting denoiser (include/ntrace_denoise.h) on the sm_100a tensor cores.
+//
+// The network's matrix products run in one GEMM kernel built on tcgen05: operand tiles are staged
+// by the CTA's threads into shared memory in the canonical K-major layout without swizzle (8 x 16-byte
+// core matrices), one elected thread issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in
+// tensor memory) and commits to an mbarrier, and the epilogue reads the accumulator back with
+// tcgen05.ld and applies a fused bias / ReLU / mask / store or atomic reduction.  Operand loaders
+// gather from any layout (row-major, transposed, or the feature stencil computed on the fly), so the
+// forward pass, the backward data products and the weight gradients (a reduction over pixels, split
+// across CTAs) all use the same kernel.  The rest (features, softmax filters, loss, bias sums, Adam)
+// are plain CUDA-core kernels.
+#include "ntrace.h"
+#include "ntrace_denoise.h"
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+namespace ntrace
+{
+int report_error(int code, const std::string& message);
+}
+
+namespace
+{
+constexpr int HID = 64;
+constexpr int TAPS = 9;
+constexpr int RADIUS = 4;
+constexpr int MAX_AXES = 5;
+
+// ------------------------------------------------------------------------------------------------
+// tcgen05 GEMM
+
+constexpr int GM = 128;      // rows per CTA: the MMA's M
+constexpr int GK = 64;       // K per shared-memory stage: 4 MMAs of K = 16
+constexpr int GTHREADS = 128;
+constexpr int SM_SMEM = 233472;  // shared memory per SM (228 KB)
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p)
+{
+        return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// byte offset of element (r, k) of a GK-wide K-major tile: core matrices of 8 rows x 16 bytes, the
+// K direction first (leading byte offset 128), then the next 8 rows (stride byte offset GK / 8 x 128)
+__device__ __forceinline__ uint32_t tile_off(int r, int k)
+{
+        return (uint32_t)((r >> 3) * (GK / 8 * 128) + (k >> 3) * 128 + (r & 7) * 16 + (k & 7) * 2);
+}
+
+// shared-memory matrix descriptor: start, leading and stride byte offsets (>> 4), version 1, no swizzle
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+        return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+               ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+
+// instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both K-major, N >> 3, M >> 4
+__host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n)
+{
+        return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ unsigned long long global_ns()
+{
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        return t;
+}
+
+// Waits for the mbarrier phase `parity` to complete; gives up after about a second.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity)
+{
+        const uint32_t addr = smem_u32(bar);
+        const unsigned long long t0 = global_ns();
+        while (true)
+        {
+                uint32_t done;
+                asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                        "selp.u32 %0, 1, 0, p;\n\t}"
+                        : "=r"(done)
+                        : "r"(addr), "r"(parity)
+                        : "memory");
+                if (done)
+                {
+                        return true;
+                }
+                if (global_ns() - t0 > 1000000000ull)
+                {
+                        return false;
+                }
+        }
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
+{
+        uint32_t r[16];
+        asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+                "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+                : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+        for (int j = 0; j < 16; ++j)
+        {
+                v[j] = __uint_as_float(r[j]);
+        }
+}
+
+// C[M x N] = sum_k A(m, k) B(n, k) over k in this CTA's K range [blockIdx.y * k_per_cta, ...).
+// LA / LB: operand loaders (float operator()(row, k), ROW_FAST: consecutive threads take consecutive
+// rows rather than consecutive k); EPI: epilogue (row, first column, 16 values).  N: multiple of 16,
+// at most 256; ncols: tensor-memory columns (power of two >= max(32, N)).
+template <class LA, class LB, class EPI>
+__global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, const EPI epi, int M, int N, int K,
+                                                   int k_per_cta, uint32_t ncols, int* err)
+{
+        extern __shared__ __align__(1024) unsigned char g_smem[];
+        __shared__ __align__(8) unsigned long long s_bar;
+        __shared__ uint32_t s_tmem;
+        unsigned char* sA = g_smem;
+        unsigned char* sB = g_smem + GM * GK * 2;
+        const int tid = threadIdx.x;
+        const int warp = tid >> 5;
+        const int lane = tid & 31;
+        const int m0 = blockIdx.x * GM;
+        const int kb = blockIdx.y * k_per_cta;
+        const int ke = min(K, kb + k_per_cta);
+
+        if (warp == 0)
+        {
+                asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
+                             "r"(ncols)
+                             : "memory");
+                asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        }
+        if (tid == 0)
+        {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)) : "memory");
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t tmem = s_tmem;
+        const uint32_t idesc = umma_idesc_bf16(GM, N);
+        const uint32_t sbo = GK / 8 * 128;
+
+        uint32_t parity = 0;
+        int stages = 0;
+        bool ok = true;
+        bool pending = false;
+        for (int kc = kb; kc < ke; kc += GK)
+        {
+                if (LA::ROW_FAST)
+                {
+                        for (int idx = tid; idx < GM * GK; idx += GTHREADS)
+                        {
+                                const int r = idx % GM, k = idx / GM;
+                                const float v = (m0 + r < M && kc + k < ke) ? la(m0 + r, kc + k) : 0.0f;
+                                *reinterpret_cast<__nv_bfloat16*>(sA + tile_off(r, k)) = __float2bfloat16_rn(v);
+                        }
+                }
+                else
+                {
+                        for (int idx = tid; idx < GM * GK; idx += GTHREADS)
+                        {
+                                const int r = idx / GK, k = idx % GK;
+                                const float v = (m0 + r < M && kc + k < ke) ? la(m0 + r, kc + k) : 0.0f;
+                                *reinterpret_cast<__nv_bfloat16*>(sA + tile_off(r, k)) = __float2bfloat16_rn(v);
+                        }
+                }
+                if (LB::ROW_FAST)
+                {
+                        for (int idx = tid; idx < N * GK; idx += GTHREADS)
+                        {
+                                const int r = idx % N, k = idx / N;
+                                const float v = (kc + k < ke) ? lb(r, kc + k) : 0.0f;
+                                *reinterpret_cast<__nv_bfloat16*>(sB + tile_off(r, k)) = __float2bfloat16_rn(v);
+                        }
+                }
+                else
+                {
+                        for (int idx = tid; idx < N * GK; idx += GTHREADS)
+                        {
+                                const int r = idx / GK, k = idx % GK;
+                                const float v = (kc + k < ke) ? lb(r, kc + k) : 0.0f;
+                                *reinterpret_cast<__nv_bfloat16*>(sB + tile_off(r, k)) = __float2bfloat16_rn(v);
+                        }
+                }
+                // the tensor core reads shared memory through the async proxy
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                __syncthreads();
+                if (tid == 0)
+                {
+                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+                        for (int s = 0; s < GK / 16; ++s)
+                        {
+                                const uint64_t da = umma_desc(smem_u32(sA) + s * 256, 128, sbo);
+                                const uint64_t db = umma_desc(smem_u32(sB) + s * 256, 128, sbo);
+                                const uint32_t accumulate = (stages > 0 || s > 0) ? 1u : 0u;
+                                asm volatile(
+                                        "{\n\t.reg .pred p;\n\t"
+                                        "setp.ne.b32 p, %4, 0;\n\t"
+                                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
+                                        "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+                                        : "memory");
+                        }
+                        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                             smem_u32(&s_bar))
+                                     : "memory");
+                }
+                pending = true;
+                // the stage is overwritten next: wait until the MMAs have read it
+                const bool done = mbar_wait(&s_bar, parity);
+                ok = __syncthreads_and(done) != 0;
+                if (!ok)
+                {
+                        break;
+                }
+                pending = false;
+                parity ^= 1u;
+                ++stages;
+        }
+        if (!ok && pending)
+        {
+                // a commit that did not arrive in time: wait once more (bounded) before the
+                // accumulator's columns are given back
+                mbar_wait(&s_bar, parity);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (ok && stages > 0)
+        {
+                const int row = m0 + warp * 32 + lane;
+                for (int c = 0; c < N; c += 16)
+                {
+                        float v[16];
+                        tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+                        if (row < M)
+                        {
+                                epi(row, c, v);
+                        }
+                }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (warp == 0)
+        {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(ncols) : "memory");
+        }
+        if (!ok && tid == 0 && err)
+        {
+                atomicOr(err, 1);
+        }
+}
+
+// ---- operand loaders ----
+
+struct LoadRows  // A(r, k) = p[r * ld + k], BF16
+{
+        static constexpr bool ROW_FAST = false;
+        const __nv_bfloat16* p;
+        int ld;
+        __device__ __forceinline__ float operator()(int r, int k) const
+        {
+                return __bfloat162float(p[(size_t)r * ld + k]);
+        }
+};
+
+struct LoadCols  // A(r, k) = p[k * ld + r], BF16 (the transpose of a row-major matrix)
+{
+        static constexpr bool ROW_FAST = true;
+        const __nv_bfloat16* p;
+        int ld;
+        __device__ __forceinline__ float operator()(int r, int k) const
+        {
+                return __bfloat162float(p[(size_t)k * ld + r]);
+        }
+};
+
+// The screen and the network's feature stencil.
+struct Stencil
+{
+        int axes;                   // n - 1
+        int size[MAX_AXES];
+        long long stride[MAX_AXES];
+        int nf;                     // base features per pixel
+        int features;               // nf x (2 axes + 1)
+
+        // pixel at offset d along axis a from p, clamped to the screen
+        __device__ __forceinline__ long long neighbour(long long p, int a, int d) const
+        {
+                const int x = (int)((p / stride[a]) % size[a]);
+                const int y = min(max(x + d, 0), size[a] - 1);
+                return p + (long long)(y - x) * stride[a];
+        }
+        // input feature k of pixel p
+        __device__ __forceinline__ float feature(const float* base, long long p, int k) const
+        {
+                if (k >= features)
+                {
+                        return 0.0f;
+                }
+                const int q = k / nf;
+                const int f = k - q * nf;
+                long long src = p;
+                if (q > 0)
+                {
+                        const int a = (q - 1) >> 1;
+                        src = neighbour(p, a, (q & 1) ? -1 : 1);
+                }
+                return base[src * nf + f];
+        }
+};
+
+struct LoadFeatures  // A(pixel, feature)
+{
+        static constexpr bool ROW_FAST = false;
+        const float* base;
+        Stencil st;
+        __device__ __forceinline__ float operator()(int r, int k) const
+        {
+                return st.feature(base, r, k);
+        }
+};
+
+struct LoadFeaturesT  // B(feature, pixel)
+{
+        static constexpr bool ROW_FAST = true;
+        const float* base;
+        Stencil st;
+        __device__ __forceinline__ float operator()(int r, int k) const
+        {
+                return st.feature(base, k, r);
+        }
+};
+
+// ---- epilogues ----
+
+struct EpiStoreF32
+{
+        float* out;
+        int ld;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                        out[(size_t)row * ld + c0 + j] = v[j];
+                }
+        }
+};
+
+struct EpiBiasF32
+{
+        const float* bias;
+        float* out;
+        int ld;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                        out[(size_t)row * ld + c0 + j] = v[j] + bias[c0 + j];
+                }
+        }
+};
+
+struct EpiBiasReluBF16
+{
+        const float* bias;
+        __nv_bfloat16* out;
+        int ld;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                        out[(size_t)row * ld + c0 + j] = __float2bfloat16_rn(fmaxf(v[j] + bias[c0 + j], 0.0f));
+                }
+        }
+};
+
+// backward through ReLU: keep the gradient where the layer's output was positive
+struct EpiMaskBF16
+{
+        const __nv_bfloat16* act;
+        __nv_bfloat16* out;
+        int ld;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                        const size_t i = (size_t)row * ld + c0 + j;
+                        out[i] = __float2bfloat16_rn(__bfloat162float(act[i]) > 0.0f ? v[j] : 0.0f);
+                }
+        }
+};
+
+// split-K partial sums added into an FP32 matrix
+struct EpiAtomicF32
+{
+        float* out;
+        int ld;
+        int ncols;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                        if (c0 + j < ncols)
+                        {
+                                atomicAdd(out + (size_t)row * ld + c0 + j, v[j]);
+                        }
+                }
+        }
+};
+
+uint32_t tmem_cols(int n)
+{
+        uint32_t c = 32;
+        while ((int)c < n)
+        {
+                c <<= 1;
+        }
+        return c;
+}
+
+template <class LA, class LB, class EPI>
+cudaError_t gemm(const LA& la, const LB& lb, const EPI& epi, int M, int N, int K, int k_per_cta, int* err,
+                 cudaStream_t st)
+{
+        if (M <= 0 || K <= 0)
+        {
+                return cudaSuccess;
+        }
+        if (N <= 0 || N % 16 != 0 || N > 256)
+        {
+                return cudaErrorInvalidValue;
+        }
+        const uint32_t ncols = tmem_cols(N);
+        // at most 512 / ncols CTAs share an SM's tensor memory: ask for enough shared memory that no
+        // more are resident (an allocation then never waits)
+        const int per_sm = 512 / (int)ncols;
+        const size_t need = (size_t)(GM + N) * GK * 2;
+        const size_t smem = std::max(need, (size_t)(SM_SMEM / (per_sm + 1) + 1024));
+        cudaError_t e = cudaFuncSetAttribute(k_gemm<LA, LB, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess)
+        {
+                return e;
+        }
+        const int kpc = k_per_cta > 0 ? (k_per_cta + GK - 1) / GK * GK : (K + GK - 1) / GK * GK;
+        dim3 grid((unsigned)((M + GM - 1) / GM), (unsigned)((K + kpc - 1) / kpc));
+        k_gemm<LA, LB, EPI><<<grid, GTHREADS, smem, st>>>(la, lb, epi, M, N, K, kpc, ncols, err);
+        return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// CUDA-core kernels
+
+constexpr int TB = 256;
+
+unsigned blocks_for(long long n)
+{
+        return (unsigned)std::min<long long>((n + TB - 1) / TB, 148LL * 64);
+}
+
+// per-pixel base features: mean (3), standard deviation of the mean (3), normal (n), depth / 10
+__global__ void k_base_features(long long P, int n, const float* __restrict__ mean, const float* __restrict__ var,
+                                const float* __restrict__ normal, const float* __restrict__ depth, float* __restrict__ out)
+{
+        const int nf = n + 7;
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
+        {
+                float* o = out + p * nf;
+                for (int c = 0; c < 3; ++c)
+                {
+                        o[c] = mean[p * 3 + c];
+                        o[3 + c] = sqrtf(fmaxf(var[p * 3 + c], 0.0f));
+                }
+                for (int k = 0; k < n; ++k)
+                {
+                        o[6 + k] = normal[p * n + k];
+                }
+                o[6 + n] = depth[p] * 0.1f;
+        }
+}
+
+__device__ __forceinline__ void softmax9(const float* z, float* w)
+{
+        float mx = z[0];
+#pragma unroll
+        for (int j = 1; j < TAPS; ++j)
+        {
+                mx = fmaxf(mx, z[j]);
+        }
+        float s = 0;
+#pragma unroll
+        for (int j = 0; j < TAPS; ++j)
+        {
+                w[j] = __expf(z[j] - mx);
+                s += w[j];
+        }
+        const float inv = 1.0f / s;
+#pragma unroll
+        for (int j = 0; j < TAPS; ++j)
+        {
+                w[j] *= inv;
+        }
+}
+
+// y_out[p] = sum_j softmax(Z[p, a*9 .. a*9+8])_j y_in[p + (j - 4) e_a]
+__global__ void k_filter_fwd(long long P, Stencil st, int a, const float* __restrict__ Z, int ldz,
+                             const float* __restrict__ y_in, float* __restrict__ y_out)
+{
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
+        {
+                float z[TAPS], w[TAPS];
+#pragma unroll
+                for (int j = 0; j < TAPS; ++j)
+                {
+                        z[j] = Z[p * ldz + a * TAPS + j];
+                }
+                softmax9(z, w);
+                float acc[3] = {0, 0, 0};
+#pragma unroll
+                for (int j = 0; j < TAPS; ++j)
+                {
+                        const long long q = st.neighbour(p, a, j - RADIUS);
+#pragma unroll
+                        for (int c = 0; c < 3; ++c)
+                        {
+                                acc[c] += w[j] * y_in[q * 3 + c];
+                        }
+                }
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                {
+                        y_out[p * 3 + c] = acc[c];
+                }
+        }
+}
+
+// backward of k_filter_fwd: dZ for the axis's taps (through the softmax) and, when g_in is given,
+// dL/dy_in added by atomics
+__global__ void k_filter_bwd(long long P, Stencil st, int a, const float* __restrict__ Z, int ldz,
+                             const float* __restrict__ y_in, const float* __restrict__ g_out, float* g_in,
+                             __nv_bfloat16* __restrict__ dZ)
+{
+        for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
+        {
+                float z[TAPS], w[TAPS], dw[TAPS];
+#pragma unroll
+                for (int j = 0; j < TAPS; ++j)
+                {
+                        z[j] = Z[p * ldz + a * TAPS + j];
+                }
+                softmax9(z, w);
+                const float g0 = g_out[p * 3], g1 = g_out[p * 3 + 1], g2 = g_out[p * 3 + 2];
+                float dot = 0;
+#pragma unroll
+                for (int j = 0; j < TAPS; ++j)
+                {
+                        const long long q = st.neighbour(p, a, j - RADIUS);
+                        dw[j] = g0 * y_in[q * 3] + g1 * y_in[q * 3 + 1] + g2 * y_in[q * 3 + 2];
+                        dot += w[j] * dw[j];
+                        if (g_in)
+                        {
+                                atomicAdd(g_in + q * 3, w[j] * g0);
+                                atomicAdd(g_in + q * 3 + 1, w[j] * g1);
+                                atomicAdd(g_in + q * 3 + 2, w[j] * g2);
+                        }
+                }
+#pragma unroll
+                for (int j = 0; j < TAPS; ++j)
+                {
+                        dZ[p * ldz + a * TAPS + j] = __float2bfloat16_rn(w[j] * (dw[j] - dot));
+                }
+        }
+}
+
+__device__ __forceinline__ double block_sum(double v, double* s_red)
+{
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1)
+        {
+                v += __shfl_down_sync(0xffffffffu, v, o);
+        }
+        if ((threadIdx.x & 31) == 0)
+        {
+                s_red[threadIdx.x >> 5] = v;
+        }
+        __syncthreads();
+        double t = 0;
+        if (threadIdx.x == 0)
+        {
+                for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+                {
+                        t += s_red[w];
+                }
+        }
+        __syncthreads();
+        return t;
+}
+
+// sums[0] += sum(target^2)
+__global__ void k_energy(long long n3, const float* __restrict__ target, double* sums)
+{
+        __shared__ double s_red[TB / 32];
+        double acc = 0;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        {
+                const double t = target[i];
+                acc += t * t;
+        }
+        const double b = block_sum(acc, s_red);
+        if (threadIdx.x == 0)
+        {
+                atomicAdd(sums, b);
+        }
+}
+
+// sums[1] += sum((out - target)^2) / sums[0]; g = 2 (out - target) / sums[0]
+__global__ void k_loss_grad(long long n3, const float* __restrict__ out, const float* __restrict__ target, double* sums,
+                            float* __restrict__ g)
+{
+        __shared__ double s_red[TB / 32];
+        const double inv = sums[0] > 0 ? 1.0 / sums[0] : 0.0;
+        double acc = 0;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        {
+                const double d = (double)out[i] - (double)target[i];
+                acc += d * d;
+                g[i] = (float)(2.0 * d * inv);
+        }
+        const double b = block_sum(acc, s_red);
+        if (threadIdx.x == 0)
+        {
+                atomicAdd(sums + 1, b * inv);
+        }
+}
+
+// out[c] += sum over rows of m[row, c] (c < cols)
+__global__ void k_colsum(long long rows, int cols, int ld, const __nv_bfloat16* __restrict__ m, float* out)
+{
+        const int c = threadIdx.x % 64;
+        const int rg = threadIdx.x / 64;
+        const int groups = blockDim.x / 64;
+        if (c >= cols)
+        {
+                return;
+        }
+        float acc = 0;
+        for (long long r = blockIdx.x * (long long)groups + rg; r < rows; r += (long long)gridDim.x * groups)
+        {
+                acc += __bfloat162float(m[r * ld + c]);
+        }
+        atomicAdd(out + c, acc);
+}
+
+__global__ void k_adam(long long count, float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
+                       float* __restrict__ v, float lr, float c1, float c2)
+{
+        const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        {
+                const float gi = g[i];
+                const float mi = b1 * m[i] + (1 - b1) * gi;
+                const float vi = b2 * v[i] + (1 - b2) * gi * gi;
+                m[i] = mi;
+                v[i] = vi;
+                w[i] -= lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+        }
+}
+
+// flat FP32 parameters -> padded BF16 weight matrices and FP32 biases for the GEMMs
+__global__ void k_pack(const float* __restrict__ w, int F, int Fp, int O, int Op, __nv_bfloat16* W1, float* b1,
+                       __nv_bfloat16* W2, float* b2, __nv_bfloat16* W3, float* b3)
+{
+        const float* w1 = w;
+        const float* pb1 = w1 + HID * F;
+        const float* w2 = pb1 + HID;
+        const float* pb2 = w2 + HID * HID;
+        const float* w3 = pb2 + HID;
+        const float* pb3 = w3 + O * HID;
+        const int total = HID * Fp + HID + HID * HID + HID + Op * HID + Op;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+        {
+                int k = i;
+                if (k < HID * Fp)
+                {
+                        const int r = k / Fp, c = k % Fp;
+                        W1[k] = __float2bfloat16_rn(c < F ? w1[r * F + c] : 0.0f);
+                        continue;
+                }
+                k -= HID * Fp;
+                if (k < HID)
+                {
+                        b1[k] = pb1[k];
+                        continue;
+                }
+                k -= HID;
+                if (k < HID * HID)
+                {
+                        W2[k] = __float2bfloat16_rn(w2[k]);
+                        continue;
+                }
+                k -= HID * HID;
+                if (k < HID)
+                {
+                        b2[k] = pb2[k];
+                        continue;
+                }
+                k -= HID;
+                if (k < Op * HID)
+                {
+                        const int r = k / HID;
+                        W3[k] = __float2bfloat16_rn(r < O ? w3[k] : 0.0f);
+                        continue;
+                }
+                k -= Op * HID;
+                b3[k] = k < O ? pb3[k] : 0.0f;
+        }
+}
+
+// padded FP32 gradients -> flat gradient in the parameter order
+__global__ void k_unpack(int F, int Fp, int O, const float* gW1, const float* gb1, const float* gW2, const float* gb2,
+                         const float* gW3, const float* gb3, float* __restrict__ g)
+{
+        const int total = HID * F + HID + HID * HID + HID + O * HID + O;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x)
+        {
+                int k = i;
+                if (k < HID * F)
+                {
+                        g[i] = gW1[(k / F) * Fp + k % F];
+                        continue;
+                }
+                k -= HID * F;
+                if (k < HID)
+                {
+                        g[i] = gb1[k];
+                        continue;
+                }
+                k -= HID;
+                if (k < HID * HID)
+                {
+                        g[i] = gW2[k];
+                        continue;
+                }
+                k -= HID * HID;
+                if (k < HID)
+                {
+                        g[i] = gb2[k];
+                        continue;
+                }
+                k -= HID;
+                if (k < O * HID)
+                {
+                        g[i] = gW3[k];
+                        continue;
+                }
+                k -= O * HID;
+                g[i] = gb3[k];
+        }
+}
+
+// ------------------------------------------------------------------------------------------------
+// host side
+
+struct DError
+{
+        int code;
+        std::string msg;
+};
+
+void ck(cudaError_t e, const char* what)
+{
+        if (e != cudaSuccess)
+        {
+                throw DError{e == cudaErrorMemoryAllocation ? NT_ENOMEM : NT_ECUDA,
+                             std::string(what) + ": " + cudaGetErrorString(e)};
+        }
+}
+
+template <typename F>
+int guard(F&& f)
+{
+        try
+        {
+                f();
+                return NT_OK;
+        }
+        catch (const DError& e)
+        {
+                return ntrace::report_error(e.code, e.msg);
+        }
+        catch (const std::bad_alloc&)
+        {
+                return ntrace::report_error(NT_ENOMEM, "host allocation failed");
+        }
+}
+
+struct Buf
+{
+        void* p = nullptr;
+        size_t bytes = 0;
+        ~Buf()
+        {
+                if (p)
+                {
+                        cudaFree(p);
+                }
+        }
+        void ensure(size_t b)
+        {
+                if (b <= bytes)
+                {
+                        return;
+                }
+                if (p)
+                {
+                        cudaFree(p);
+                        p = nullptr;
+                        bytes = 0;
+                }
+                ck(cudaMalloc(&p, b), "cudaMalloc");
+                bytes = b;
+        }
+        template <typename T>
+        T* as() const
+        {
+                return static_cast<T*>(p);
+        }
+};
+
+uint64_t splitmix(uint64_t& s)
+{
+        uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        return z ^ (z >> 31);
+}
+}
+
+struct nt_denoiser
+{
+        int n = 0;
+        int nf = 0, F = 0, Fp = 0, O = 0, Op = 0;
+        long long nparams = 0;
+        long long P = 0;
+        Stencil st{};
+        cudaStream_t own = nullptr;
+        cudaStream_t st_use = nullptr;
+        long long adam_t = 0;
+        // parameters and optimiser state (flat FP32), packed weights
+        Buf w, g, m, v;
+        Buf W1, b1, W2, b2, W3, b3;
+        // padded FP32 gradients in one block (cleared together): gW1 | gb1 | gW2 | gb2 | gW3 | gb3
+        Buf gblock;
+        float *gW1 = nullptr, *gb1 = nullptr, *gW2 = nullptr, *gb2 = nullptr, *gW3 = nullptr, *gb3 = nullptr;
+        // per-image workspace
+        Buf base, H1, H2, Z, Y, G, dZ, dH1, dH2, sums, err;
+        bool packed = false;
+
+        size_t gbytes() const
+        {
+                return sizeof(float) * (size_t)(HID * Fp + HID + HID * HID + HID + Op * HID + Op);
+        }
+};
+
+namespace
+{
+void pack(nt_denoiser* d)
+{
+        k_pack<<<64, TB, 0, d->st_use>>>(d->w.as<float>(), d->F, d->Fp, d->O, d->Op, d->W1.as<__nv_bfloat16>(),
+                                         d->b1.as<float>(), d->W2.as<__nv_bfloat16>(), d->b2.as<float>(),
+                                         d->W3.as<__nv_bfloat16>(), d->b3.as<float>());
+        ck(cudaGetLastError(), "pack");
+        d->packed = true;
+}
+
+void check_err(nt_denoiser* d)
+{
+        int h = 0;
+        ck(cudaMemcpyAsync(&h, d->err.p, sizeof(int), cudaMemcpyDeviceToHost, d->st_use), "error flag");
+        ck(cudaStreamSynchronize(d->st_use), "sync");
+        if (h)
+        {
+                throw DError{NT_ETIMEOUT, "tensor-core GEMM: an MMA completion wait ran out"};
+        }
+}
+
+// forward pass of the current input: Y[n-1] is the denoised image
+void forward(nt_denoiser* d)
+{
+        if (d->P <= 0)
+        {
+                throw DError{NT_ESTATE, "no input set"};
+        }
+        if (!d->packed)
+        {
+                pack(d);
+        }
+        const long long P = d->P;
+        const int P32 = (int)P;
+        cudaStream_t s = d->st_use;
+        int* err = d->err.as<int>();
+        ck(gemm(LoadFeatures{d->base.as<float>(), d->st}, LoadRows{d->W1.as<__nv_bfloat16>(), d->Fp},
+                EpiBiasReluBF16{d->b1.as<float>(), d->H1.as<__nv_bfloat16>(), HID}, P32, HID, d->Fp, 0, err, s),
+           "gemm 1");
+        ck(gemm(LoadRows{d->H1.as<__nv_bfloat16>(), HID}, LoadRows{d->W2.as<__nv_bfloat16>(), HID},
+                EpiBiasReluBF16{d->b2.as<float>(), d->H2.as<__nv_bfloat16>(), HID}, P32, HID, HID, 0, err, s),
+           "gemm 2");
+        ck(gemm(LoadRows{d->H2.as<__nv_bfloat16>(), HID}, LoadRows{d->W3.as<__nv_bfloat16>(), HID},
+                EpiBiasF32{d->b3.as<float>(), d->Z.as<float>(), d->Op}, P32, d->Op, HID, 0, err, s),
+           "gemm 3");
+        for (int a = 0; a < d->n - 1; ++a)
+        {
+                k_filter_fwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->Z.as<float>(), d->Op,
+                                                            d->Y.as<float>() + (size_t)a * P * 3,
+                                                            d->Y.as<float>() + (size_t)(a + 1) * P * 3);
+        }
+        ck(cudaGetLastError(), "filter");
+}
+
+// loss and gradients (padded, in gW*/gb*) against target
+double backward(nt_denoiser* d, const float* target)
+{
+        const long long P = d->P;
+        const int P32 = (int)P;
+        cudaStream_t s = d->st_use;
+        int* err = d->err.as<int>();
+        const int A = d->n - 1;
+        ck(cudaMemsetAsync(d->sums.p, 0, 2 * sizeof(double), s), "memset");
+        k_energy<<<blocks_for(P * 3), TB, 0, s>>>(P * 3, target, d->sums.as<double>());
+        float* G0 = d->G.as<float>();
+        float* G1 = G0 + (size_t)P * 3;
+        k_loss_grad<<<blocks_for(P * 3), TB, 0, s>>>(P * 3, d->Y.as<float>() + (size_t)A * P * 3, target,
+                                                       d->sums.as<double>(), G0);
+        ck(cudaMemsetAsync(d->dZ.p, 0, (size_t)P * d->Op * sizeof(__nv_bfloat16), s), "memset");
+        float* gout = G0;
+        float* gin = G1;
+        for (int a = A - 1; a >= 0; --a)
+        {
+                if (a > 0)
+                {
+                        ck(cudaMemsetAsync(gin, 0, (size_t)P * 3 * sizeof(float), s), "memset");
+                }
+                k_filter_bwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->Z.as<float>(), d->Op,
+                                                            d->Y.as<float>() + (size_t)a * P * 3, gout, a > 0 ? gin : nullptr,
+                                                            d->dZ.as<__nv_bfloat16>());
+                std::swap(gout, gin);
+        }
+        ck(cudaGetLastError(), "filter backward");
+        // backward data products
+        ck(gemm(LoadRows{d->dZ.as<__nv_bfloat16>(), d->Op}, LoadCols{d->W3.as<__nv_bfloat16>(), HID},
+                EpiMaskBF16{d->H2.as<__nv_bfloat16>(), d->dH2.as<__nv_bfloat16>(), HID}, P32, HID, d->Op, 0, err, s),
+           "gemm dH2");
+        ck(gemm(LoadRows{d->dH2.as<__nv_bfloat16>(), HID}, LoadCols{d->W2.as<__nv_bfloat16>(), HID},
+                EpiMaskBF16{d->H1.as<__nv_bfloat16>(), d->dH1.as<__nv_bfloat16>(), HID}, P32, HID, HID, 0, err, s),
+           "gemm dH1");
+        // weight gradients: reductions over pixels, split across CTAs
+        ck(cudaMemsetAsync(d->gblock.p, 0, d->gbytes(), s), "memset");
+        const int kpc = 4096;
+        ck(gemm(LoadCols{d->dZ.as<__nv_bfloat16>(), d->Op}, LoadCols{d->H2.as<__nv_bfloat16>(), HID},
+                EpiAtomicF32{d->gW3, HID, HID}, d->Op, HID, P32, kpc, err, s),
+           "gemm dW3");
+        ck(gemm(LoadCols{d->dH2.as<__nv_bfloat16>(), HID}, LoadCols{d->H1.as<__nv_bfloat16>(), HID},
+                EpiAtomicF32{d->gW2, HID, HID}, HID, HID, P32, kpc, err, s),
+           "gemm dW2");
+        ck(gemm(LoadCols{d->dH1.as<__nv_bfloat16>(), HID}, LoadFeaturesT{d->base.as<float>(), d->st},
+                EpiAtomicF32{d->gW1, d->Fp, d->Fp}, HID, d->Fp, P32, kpc, err, s),
+           "gemm dW1");
+        const unsigned cb = (unsigned)std::min<long long>((P + 3) / 4, 1024);
+        k_colsum<<<cb, TB, 0, s>>>(P, d->Op, d->Op, d->dZ.as<__nv_bfloat16>(), d->gb3);
+        k_colsum<<<cb, TB, 0, s>>>(P, HID, HID, d->dH2.as<__nv_bfloat16>(), d->gb2);
+        k_colsum<<<cb, TB, 0, s>>>(P, HID, HID, d->dH1.as<__nv_bfloat16>(), d->gb1);
+        k_unpack<<<64, TB, 0, s>>>(d->F, d->Fp, d->O, d->gW1, d->gb1, d->gW2,
+                                   d->gb2, d->gW3, d->gb3, d->g.as<float>());
+        ck(cudaGetLastError(), "gradients");
+        double sums[2];
+        ck(cudaMemcpyAsync(sums, d->sums.p, sizeof(sums), cudaMemcpyDeviceToHost, s), "loss");
+        check_err(d);
+        return sums[1];
+}
+}
+
+extern "C" {
+
+int nt_denoiser_create(int n, uint64_t seed, nt_denoiser** out)
+{
+        return guard([&]() {
+                if (!out || n < 3 || n > 6)
+                {
+                        throw DError{NT_EINVAL, "n must be 3..6"};
+                }
+                auto d = std::make_unique<nt_denoiser>();
+                d->n = n;
+                d->nf = n + 7;
+                d->F = d->nf * (2 * (n - 1) + 1);
+                d->Fp = (d->F + 15) / 16 * 16;
+                d->O = TAPS * (n - 1);
+                d->Op = (d->O + 15) / 16 * 16;
+                d->nparams = (long long)HID * d->F + HID + HID * HID + HID + (long long)d->O * HID + d->O;
+                ck(cudaStreamCreateWithFlags(&d->own, cudaStreamNonBlocking), "cudaStreamCreate");
+                d->st_use = d->own;
+                const size_t pb = sizeof(float) * (size_t)d->nparams;
+                d->w.ensure(pb);
+                d->g.ensure(pb);
+                d->m.ensure(pb);
+                d->v.ensure(pb);
+                ck(cudaMemsetAsync(d->m.p, 0, pb, d->own), "memset");
+                ck(cudaMemsetAsync(d->v.p, 0, pb, d->own), "memset");
+                d->W1.ensure(sizeof(__nv_bfloat16) * HID * d->Fp);
+                d->b1.ensure(sizeof(float) * HID);
+                d->W2.ensure(sizeof(__nv_bfloat16) * HID * HID);
+                d->b2.ensure(sizeof(float) * HID);
+                d->W3.ensure(sizeof(__nv_bfloat16) * d->Op * HID);
+                d->b3.ensure(sizeof(float) * d->Op);
+                d->gblock.ensure(d->gbytes());
+                d->gW1 = d->gblock.as<float>();
+                d->gb1 = d->gW1 + HID * d->Fp;
+                d->gW2 = d->gb1 + HID;
+                d->gb2 = d->gW2 + HID * HID;
+                d->gW3 = d->gb2 + HID;
+                d->gb3 = d->gW3 + d->Op * HID;
+                d->sums.ensure(2 * sizeof(double));
+                d->err.ensure(sizeof(int));
+                ck(cudaMemsetAsync(d->err.p, 0, sizeof(int), d->own), "memset");
+                // initial weights: Kaiming-uniform hidden layers, a small output layer, zero biases
+                std::vector<float> h((size_t)d->nparams, 0.0f);
+                uint64_t s = seed;
+                auto uni = [&](float bound) {
+                        const double u = (double)(splitmix(s) >> 11) * (1.0 / 9007199254740992.0);
+                        return (float)((2 * u - 1) * bound);
+                };
+                size_t k = 0;
+                const float bw1 = std::sqrt(6.0f / d->F), bw2 = std::sqrt(6.0f / HID), bw3 = 0.1f * std::sqrt(6.0f / HID);
+                for (int i = 0; i < HID * d->F; ++i)
+                {
+                        h[k++] = uni(bw1);
+                }
+                k += HID;
+                for (int i = 0; i < HID * HID; ++i)
+                {
+                        h[k++] = uni(bw2);
+                }
+                k += HID;
+                for (int i = 0; i < d->O * HID; ++i)
+                {
+                        h[k++] = uni(bw3);
+                }
+                ck(cudaMemcpyAsync(d->w.p, h.data(), pb, cudaMemcpyHostToDevice, d->own), "upload");
+                ck(cudaStreamSynchronize(d->own), "sync");
+                *out = d.release();
+        });
+}
+
+int nt_denoiser_destroy(nt_denoiser* d)
+{
+        if (!d)
+        {
+                return NT_OK;
+        }
+        if (d->own)
+        {
+                cudaStreamSynchronize(d->own);
+                cudaStreamDestroy(d->own);
+        }
+        delete d;
+        return NT_OK;
+}
+
+int nt_denoiser_get_layout(nt_denoiser* d, nt_denoiser_layout* out)
+{
+        return guard([&]() {
+                if (!d || !out)
+                {
+                        throw DError{NT_EINVAL, "null argument"};
+                }
+                out->n = d->n;
+                out->base_features = d->nf;
+                out->features = d->F;
+                out->features_padded = d->Fp;
+                out->hidden = HID;
+                out->outputs = d->O;
+                out->outputs_padded = d->Op;
+                out->param_count = d->nparams;
+        });
+}
+
+int nt_denoiser_get_params(nt_denoiser* d, float* params)
+{
+        return guard([&]() {
+                if (!d || !params)
+                {
+                        throw DError{NT_EINVAL, "null argument"};
+                }
+                ck(cudaMemcpyAsync(params, d->w.p, sizeof(float) * d->nparams, cudaMemcpyDeviceToHost, d->st_use), "copy");
+                ck(cudaStreamSynchronize(d->st_use), "sync");
+        });
+}
+
+int nt_denoiser_set_params(nt_denoiser* d, const float* params)
+{
+        return guard([&]() {
+                if (!d || !params)
+                {
+                        throw DError{NT_EINVAL, "null argument"};
+                }
+                ck(cudaMemcpyAsync(d->w.p, params, sizeof(float) * d->nparams, cudaMemcpyHostToDevice, d->st_use), "copy");
+                ck(cudaStreamSynchronize(d->st_use), "sync");
+                d->packed = false;
+        });
+}
+
+int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, const float* d_mean, const float* d_var,
+                          const float* d_normal, const float* d_depth, void* stream)
+{
+        return guard([&]() {
+                if (!d || !screen || !d_mean || !d_var || !d_normal || !d_depth)
+                {
+                        throw DError{NT_EINVAL, "null argument"};
+                }
+                Stencil st{};
+                st.axes = d->n - 1;
+                long long P = 1;
+                for (int a = 0; a < st.axes; ++a)
+                {
+                        if (screen[a] < 1)
+                        {
+                                throw DError{NT_EINVAL, "screen sizes must be positive"};
+                        }
+                        st.size[a] = screen[a];
+                        st.stride[a] = P;
+                        P *= screen[a];
+                }
+                if (P > (1LL << 30))
+                {
+                        throw DError{NT_EINVAL, "too many pixels for the denoiser"};
+                }
+                st.nf = d->nf;
+                st.features = d->F;
+                d->st = st;
+                d->P = P;
+                d->st_use = stream ? (cudaStream_t)stream : d->own;
+                d->base.ensure(sizeof(float) * (size_t)P * d->nf);
+                d->H1.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
+                d->H2.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
+                d->dH1.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
+                d->dH2.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
+                d->Z.ensure(sizeof(float) * (size_t)P * d->Op);
+                d->dZ.ensure(sizeof(__nv_bfloat16) * (size_t)P * d->Op);
+                d->Y.ensure(sizeof(float) * (size_t)P * 3 * d->n);
+                d->G.ensure(sizeof(float) * (size_t)P * 3 * 2);
+                k_base_features<<<blocks_for(P), TB, 0, d->st_use>>>(P, d->n, d_mean, d_var, d_normal, d_depth,
+                                                                      d->base.as<float>());
+                ck(cudaGetLastError(), "features");
+                ck(cudaMemcpyAsync(d->Y.p, d_mean, sizeof(float) * (size_t)P * 3, cudaMemcpyDeviceToDevice, d->st_use),
+                   "copy");
+        });
+}
+
+int nt_denoiser_apply(nt_denoiser* d, float* d_out)
+{
+        return guard([&]() {
+                if (!d || !d_out)
+                {
+                        throw DError{NT_EINVAL, "null argument"};
+                }
+                forward(d);
+                ck(cudaMemcpyAsync(d_out, d->Y.as<float>() + (size_t)(d->n - 1) * d->P * 3, sizeof(float) * (size_t)d->P * 3,
+                                   cudaMemcpyDeviceToDevice, d->st_use),
+                   "copy");
+                check_err(d);
+        });
+}
+
+int nt_denoiser_gradient(nt_denoiser* d, const float* d_target, float* grad, double* loss)
+{
+        return guard([&]() {
+                if (!d || !d_target)
+                {
+                        throw DError{NT_EINVAL, "null argument"};
+                }
+                forward(d);
+                const double l = backward(d, d_target);
+                if (grad)
+                {
+                        ck(cudaMemcpyAsync(grad, d->g.p, sizeof(float) * d->nparams, cudaMemcpyDeviceToHost, d->st_use),
+                           "copy");
+                        ck(cudaStreamSynchronize(d->st_use), "sync");
+                }
+                if (loss)
+                {
+                        *loss = l;
+                }
+        });
+}
+
+int nt_denoiser_train_step(nt_denoiser* d, const float* d_target, float lr, double* loss)
+{
+        return guard([&]() {
+                if (!d || !d_target || !(lr > 0))
+                {
+                        throw DError{NT_EINVAL, "bad argument"};
+                }
+                forward(d);
+                const double l = backward(d, d_target);
+                ++d->adam_t;
+                const float c1 = 1.0f - std::pow(0.9f, (float)d->adam_t);
+                const float c2 = 1.0f - std::pow(0.999f, (float)d->adam_t);
+                k_adam<<<blocks_for(d->nparams), TB, 0, d->st_use>>>(d->nparams, d->w.as<float>(), d->g.as<float>(),
+                                                                     d->m.as<float>(), d->v.as<float>(), lr, c1, c2);
+                ck(cudaGetLastError(), "adam");
+                pack(d);
+                if (loss)
+                {
+                        *loss = l;
+                }
+        });
+}
+
+int nt_tc_gemm_bf16(const uint16_t* d_a, const uint16_t* d_b, float* d_c, int m, int n, int k, void* stream)
+{
+        return guard([&]() {
+                if (!d_a || !d_b || !d_c || m < 1 || n < 16 || n > 256 || n % 16 || k < 16 || k % 16)
+                {
+                        throw DError{NT_EINVAL, "nt_tc_gemm_bf16: bad arguments"};
+                }
+                cudaStream_t s = (cudaStream_t)stream;
+                Buf err;
+                err.ensure(sizeof(int));
+                ck(cudaMemsetAsync(err.p, 0, sizeof(int), s), "memset");
+                ck(gemm(LoadRows{(const __nv_bfloat16*)d_a, k}, LoadRows{(const __nv_bfloat16*)d_b, k}, EpiStoreF32{d_c, n},
+                        m, n, k, 0, err.as<int>(), s),
+                   "gemm");
+                int h = 0;
+                ck(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+                ck(cudaStreamSynchronize(s), "sync");
+                if (h)
+                {
+                        throw DError{NT_ETIMEOUT, "tensor-core GEMM: an MMA completion wait ran out"};
+                }
+        });
+}
+}

@@ -18,9 +18,10 @@ static_assert(BLOCK == WALK_BLOCK, "path-cache slots are laid out for the walk k
 #define NT_WALK_MIN_BLOCKS 2
 #endif
 constexpr int WALK_MIN_BLOCKS = NT_WALK_MIN_BLOCKS;
-// fill rounds per iteration of the lane-refill walks
+// fill rounds per iteration of the lane-refill walks (1 measured faster than 2, 4, 8 or 16: a lane
+// whose new ray needs no walk waits for the next iteration rather than holding up the warp)
 #ifndef NT_FILL_ROUNDS
-#define NT_FILL_ROUNDS 8
+#define NT_FILL_ROUNDS 1
 #endif
 constexpr int FILL_ROUNDS = NT_FILL_ROUNDS;
 
@@ -782,6 +783,126 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         flush_stats<true>(counters, ws, 0, rays);
 }
 
+// ------------------------------------------------------------------------------------------------
+// Denoiser inputs
+
+// First hit of the pixel-centre camera ray: geometric normal turned towards the camera (as the
+// shading normal of trace_path, painter.cpp:369-373) and distance; zeros on a miss.
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_aux(__grid_constant__ const DevScene<N> S, long long npix,
+                                               float* __restrict__ normal, float* __restrict__ depth)
+{
+        const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        WalkStats ws{0, 0, 0, 0, 0};
+        if (i >= npix)
+        {
+                return;
+        }
+        float point[N - 1];
+        long long rem = i;
+#pragma unroll
+        for (int j = 0; j < N - 1; ++j)
+        {
+                point[j] = (float)(rem % S.proj.screen[j]) + 0.5f;
+                rem /= S.proj.screen[j];
+        }
+        Ray<N> ray;
+        projector_ray<N>(S.proj, point, ray);
+        float t;
+        int obj, facet;
+        float gn[N];
+        float d = 0;
+        if (scene_closest<N>(S, ray, &t, &obj, &facet, &ws))
+        {
+                float p[N];
+                ray_point<N>(ray, t, p);
+                const ObjDev& ob = S.obj[obj];
+                if (ob.kind == OBJ_MESH)
+                {
+                        const float4* rec = S.mesh[ob.index].rec32 + (size_t)facet * Rec32<N>::F4;
+                        float f4[(N + 3) / 4 * 4];
+#pragma unroll
+                        for (int q = 0; q < (N + 3) / 4; ++q)
+                        {
+                                float4 v = __ldg(rec + q);
+                                f4[4 * q + 0] = v.x;
+                                f4[4 * q + 1] = v.y;
+                                f4[4 * q + 2] = v.z;
+                                f4[4 * q + 3] = v.w;
+                        }
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                gn[k] = f4[k];
+                        }
+                }
+                else if (ob.kind == OBJ_PLT)
+                {
+                        plt_normal<N>(S.plt[ob.index], p, gn);
+                }
+                else
+                {
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                gn[k] = S.hplt[ob.index].normal[k];
+                        }
+                }
+                vnormalize<N>(gn);
+                if (vdot<N>(ray.dir, gn) > 0)
+                {
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                gn[k] = -gn[k];
+                        }
+                }
+                d = t;
+        }
+        else
+        {
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        gn[k] = 0;
+                }
+        }
+#pragma unroll
+        for (int k = 0; k < N; ++k)
+        {
+                normal[i * N + k] = gn[k];
+        }
+        depth[i] = d;
+}
+
+// sum += v, sumsq += v^2 for the per-pixel values v of a single-sample pass
+__global__ void k_moments_add(long long n3, const double* __restrict__ accum, float* __restrict__ sum,
+                              float* __restrict__ sumsq)
+{
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        {
+                const float v = (float)accum[i];
+                sum[i] += v;
+                sumsq[i] += v * v;
+        }
+}
+
+// sums of `passes` samples -> mean and the variance of the mean (sample variance / passes)
+__global__ void k_moments_finish(long long n3, int passes, float* __restrict__ mean, float* __restrict__ var)
+{
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        {
+                const float m = mean[i] / passes;
+                float v = 0;
+                if (passes > 1)
+                {
+                        v = fmaxf(var[i] - passes * m * m, 0.0f) / (float)(passes - 1) / (float)passes;
+                }
+                mean[i] = m;
+                var[i] = v;
+        }
+}
+
 template <int N>
 long long grid_for(long long count)
 {
@@ -976,10 +1097,42 @@ cudaError_t launch_trace_closest(const MeshDev<N>& M, const float* org, const fl
         return cudaGetLastError();
 }
 
+template <int N>
+cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, float* depth, cudaStream_t st)
+{
+        if (npix <= 0)
+        {
+                return cudaSuccess;
+        }
+        k_aux<N><<<(unsigned)grid_for<N>(npix), BLOCK, 0, st>>>(S, npix, normal, depth);
+        return cudaGetLastError();
+}
+
+cudaError_t launch_moments_add(long long n3, const double* accum, float* sum, float* sumsq, cudaStream_t st)
+{
+        const unsigned g = (unsigned)std::min<long long>((n3 + BLOCK - 1) / BLOCK, 148LL * 32);
+        if (n3 > 0)
+        {
+                k_moments_add<<<g, BLOCK, 0, st>>>(n3, accum, sum, sumsq);
+        }
+        return cudaGetLastError();
+}
+
+cudaError_t launch_moments_finish(long long n3, int passes, float* mean, float* var, cudaStream_t st)
+{
+        const unsigned g = (unsigned)std::min<long long>((n3 + BLOCK - 1) / BLOCK, 148LL * 32);
+        if (n3 > 0)
+        {
+                k_moments_finish<<<g, BLOCK, 0, st>>>(n3, passes, mean, var);
+        }
+        return cudaGetLastError();
+}
+
 #define NT_INSTANTIATE(N)                                                                                         \
         template struct Wavefront<N>;                                                                             \
         template cudaError_t launch_trace_closest<N>(const MeshDev<N>&, const float*, const float*, long long, int, \
-                                                     int*, float*, unsigned long long*, cudaStream_t);
+                                                     int*, float*, unsigned long long*, cudaStream_t);          \
+        template cudaError_t launch_aux<N>(const DevScene<N>&, long long, float*, float*, cudaStream_t);
 NT_INSTANTIATE(3)
 NT_INSTANTIATE(4)
 NT_INSTANTIATE(5)

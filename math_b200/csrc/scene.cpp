@@ -236,6 +236,10 @@ struct MeshHost
         // pinned host copy of the four device arrays, back to back (re-upload, nt_scene_upload)
         void* pinned = nullptr;
         size_t pinned_bytes = 0;
+        // facet setup and tree done / device arrays current: a rebuild after edits that leave the
+        // mesh unchanged (lights, surfaces, projector) reuses both
+        bool ready = false;
+        bool uploaded = false;
 
         MeshHost() = default;
         MeshHost(const MeshHost&) = delete;
@@ -247,7 +251,7 @@ struct MeshHost
                   dist(o.dist), vmin(std::move(o.vmin)), vmax(std::move(o.vmax)), leaf_count(o.leaf_count),
                   degenerate(o.degenerate), build_seconds(o.build_seconds), d_rec32(std::move(o.d_rec32)),
                   d_rec64(std::move(o.d_rec64)), d_nodes(std::move(o.d_nodes)), d_idx(std::move(o.d_idx)),
-                  pinned(o.pinned), pinned_bytes(o.pinned_bytes)
+                  pinned(o.pinned), pinned_bytes(o.pinned_bytes), ready(o.ready), uploaded(o.uploaded)
         {
                 o.pinned = nullptr;
                 o.pinned_bytes = 0;
@@ -895,8 +899,13 @@ void build_scene(nt_scene* s, unsigned threads, bool host_only)
         }
         for (auto& m : s->meshes)
         {
-                build_mesh<N>(m, threads);
-                if (!host_only)
+                if (!m.ready)
+                {
+                        build_mesh<N>(m, threads);
+                        m.ready = true;
+                        m.uploaded = false;
+                }
+                if (!host_only && !m.uploaded)
                 {
                         m.d_rec32.upload(m.rec32, s->stream);
                         m.d_rec64.upload(m.rec64, s->stream);
@@ -918,6 +927,7 @@ void build_scene(nt_scene* s, unsigned threads, bool host_only)
                         std::memcpy(p, m.nodes.data(), m.d_nodes.bytes);
                         p += m.d_nodes.bytes;
                         std::memcpy(p, m.leaf_idx.data(), m.d_idx.bytes);
+                        m.uploaded = true;
                 }
         }
         for (auto& p : s->plts)
@@ -1426,6 +1436,16 @@ struct RenderF
         }
 };
 template <int N>
+struct AuxF
+{
+        static void run(nt_scene* s, float* normal, float* depth, cudaStream_t st)
+        {
+                DevScene<N> S;
+                std::memcpy(&S, s->dev_scene.data(), sizeof(S));
+                check_cuda(launch_aux<N>(S, s->pixel_count(), normal, depth, st), "aux");
+        }
+};
+template <int N>
 struct TraceF
 {
         static void run(nt_scene* s, int mi, const float* o, const float* d, long long nr, int rt, int* f, float* t,
@@ -1734,6 +1754,40 @@ int nt_scene_set_background(nt_scene* scene, const nt_surface* surface)
         });
 }
 
+int nt_scene_clear_lights(nt_scene* scene)
+{
+        return guarded([&]() {
+                need_scene(scene);
+                scene->lights.clear();
+                scene->built = false;
+        });
+}
+
+int nt_scene_set_object_surface(nt_scene* scene, int object, const nt_surface* surface)
+{
+        return guarded([&]() {
+                need_scene(scene);
+                if (!surface || object < 0 || object >= (int)scene->objects.size())
+                {
+                        fail(NT_EINVAL, "bad object index or surface");
+                }
+                const ObjRef& o = scene->objects[object];
+                if (o.kind == OBJ_MESH)
+                {
+                        scene->meshes[o.index].surface = *surface;
+                }
+                else if (o.kind == OBJ_PLT)
+                {
+                        scene->plts[o.index].surface = *surface;
+                }
+                else
+                {
+                        scene->hplts[o.index].surface = *surface;
+                }
+                scene->built = false;
+        });
+}
+
 int nt_scene_build(nt_scene* scene, const nt_build_opts* opts)
 {
         return guarded([&]() {
@@ -1862,6 +1916,63 @@ int nt_render(nt_scene* scene, const nt_render_opts* opts, nt_stats* stats)
                         fail(NT_EINVAL, "opts is NULL");
                 }
                 dispatch<RenderF>(scene->n, scene, *opts, stats);
+        });
+}
+
+int nt_render_aux(nt_scene* scene, float* d_normal, float* d_depth, void* stream)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!d_normal || !d_depth)
+                {
+                        fail(NT_EINVAL, "null output array");
+                }
+                cudaStream_t st = stream ? (cudaStream_t)stream : scene->stream;
+                dispatch<AuxF>(scene->n, scene, d_normal, d_depth, st);
+                check_cuda(cudaStreamSynchronize(st), "aux sync");
+        });
+}
+
+int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int passes, int64_t sample_offset, float* d_mean,
+                      float* d_var, nt_stats* stats)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!opts || passes < 1 || sample_offset < 0 || !d_mean || !d_var)
+                {
+                        fail(NT_EINVAL, "bad moments arguments");
+                }
+                const long long n3 = scene->pixel_count() * 3;
+                check_cuda(cudaMemsetAsync(d_mean, 0, n3 * sizeof(float), scene->stream), "memset");
+                check_cuda(cudaMemsetAsync(d_var, 0, n3 * sizeof(float), scene->stream), "memset");
+                nt_render_opts o = *opts;
+                o.samples_per_pixel = 1;
+                nt_stats total{};
+                for (int p = 0; p < passes; ++p)
+                {
+                        check_cuda(cudaMemsetAsync(scene->accum.p, 0, scene->accum.bytes, scene->stream), "memset");
+                        scene->samples_done = sample_offset + p;
+                        nt_stats one{};
+                        dispatch<RenderF>(scene->n, scene, o, &one);
+                        check_cuda(launch_moments_add(n3, scene->accum.as<double>(), d_mean, d_var, scene->stream), "moments");
+                        total.paths += one.paths;
+                        total.rays += one.rays;
+                        total.shadow_rays += one.shadow_rays;
+                        total.facet_tests += one.facet_tests;
+                        total.box_steps += one.box_steps;
+                        total.retests += one.retests;
+                        total.descent_levels += one.descent_levels;
+                        total.error_bits |= one.error_bits;
+                        total.launches += one.launches + 1;
+                        total.seconds += one.seconds;
+                }
+                check_cuda(launch_moments_finish(n3, passes, d_mean, d_var, scene->stream), "moments");
+                check_cuda(cudaStreamSynchronize(scene->stream), "moments sync");
+                total.spp_effective = passes;
+                if (stats)
+                {
+                        *stats = total;
+                }
         });
 }
 

@@ -33,7 +33,11 @@ EXPORTED_SYMBOLS = (
     "nt_scene_set_projector", "nt_scene_set_background", "nt_scene_build", "nt_scene_mesh_info", "nt_render",
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
-    "nt_scene_upload", "nt_scene_stream",
+    "nt_scene_upload", "nt_scene_stream", "nt_scene_clear_lights", "nt_scene_set_object_surface", "nt_render_aux",
+    "nt_render_moments", "nt_render_noalloc",
+    "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
+    "nt_denoiser_set_params", "nt_denoiser_set_input", "nt_denoiser_apply", "nt_denoiser_gradient",
+    "nt_denoiser_train_step", "nt_tc_gemm_bf16",
 )
 
 
@@ -126,6 +130,11 @@ def library() -> ctypes.CDLL:
         "nt_last_error_message": ([], ctypes.c_char_p),
         "nt_effective_spp": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "nt_cosine_sphere_coefficient": ([ctypes.c_int], ctypes.c_double),
+        "nt_scene_clear_lights": ([vp], ctypes.c_int),
+        "nt_scene_set_object_surface": ([vp, ctypes.c_int, ctypes.POINTER(Surface)], ctypes.c_int),
+        "nt_render_aux": ([vp, vp, vp, vp], ctypes.c_int),
+        "nt_render_moments": ([vp, ctypes.POINTER(RenderOpts), ctypes.c_int, i64, vp, vp, ctypes.POINTER(Stats)],
+                              ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -296,6 +305,28 @@ class Scene:
         spp = ctypes.c_int64()
         _check(self._lib.nt_accum_read(self._h, out.ctypes.data, ctypes.byref(spp)))
         return out, int(spp.value)
+
+    def clear_lights(self) -> None:
+        """Removes every light (add new ones, then build again; the meshes' trees are kept)."""
+        _check(self._lib.nt_scene_clear_lights(self._h))
+
+    def set_object_surface(self, obj: int, color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False,
+                           light_color=(0.0, 0.0, 0.0)) -> None:
+        s = _surface(color, diffuse, light_source, light_color)
+        _check(self._lib.nt_scene_set_object_surface(self._h, int(obj), ctypes.byref(s)))
+
+    def render_aux(self, d_normal: int, d_depth: int, stream: int = 0) -> None:
+        """First-hit normal (pixels x n) and depth (pixels) into device arrays (pointers as integers)."""
+        _check(self._lib.nt_render_aux(self._h, d_normal, d_depth, stream or None))
+
+    def render_moments(self, passes: int, d_mean: int, d_var: int, sample_offset: int = 0, max_depth: int = 100,
+                       seed: int = 0, retest: bool = True) -> dict:
+        """`passes` single-sample passes: per-pixel mean and variance of the mean into device arrays."""
+        o = RenderOpts(1, int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)), 0, 0, 0, None)
+        st = Stats()
+        _check(self._lib.nt_render_moments(self._h, ctypes.byref(o), int(passes), int(sample_offset), d_mean, d_var,
+                                           ctypes.byref(st)))
+        return st.as_dict()
 
     def trace_closest(self, org, dirs, mesh_index: int = 0, retest: bool = True):
         """Closest facet per ray (-1 = miss) and distance; plus the call's statistics."""

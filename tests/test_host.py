@@ -1,4 +1,4 @@
-"""Host side of the product library, without a GPU: the C ABI loads and exports what include/ntrace.h
+"""Host side of the product library, without a GPU: the C ABI loads and exports what include/*.h
 declares, the multithreaded float tree build reproduces the reference's Mesh<N,float> tree (as
 restated by the oracle, itself pinned to the reference), and malformed scenes are rejected with the
 documented status codes before anything is launched."""
@@ -13,7 +13,7 @@ from conftest import GOLDEN, ROOT
 
 
 def _header_functions():
-    text = (ROOT / "include" / "ntrace.h").read_text()
+    text = "\n".join(h.read_text() for h in sorted((ROOT / "include").glob("*.h")))
     return sorted(set(re.findall(r"^\s*(?:const\s+)?[A-Za-z_][A-Za-z0-9_ ]*\*?\s+\**(nt_[a-z0-9_]+)\s*\(", text, re.M)))
 
 
