@@ -196,12 +196,12 @@ int nt_accum_clear(nt_scene* scene);
  * into device arrays.  stream: a cudaStream_t, NULL for the scene's stream. */
 int nt_render_aux(nt_scene* scene, float* d_normal, float* d_depth, void* stream);
 
-/* `passes` single-sample passes (sample indices sample_offset, sample_offset + 1, ...; opts gives the
- * seed, depth and re-test, its samples_per_pixel is ignored) and, per pixel, the mean radiance and
- * the variance of that mean (sample variance / passes; 0 for one pass), into device arrays of
- * pixel_count x 3 floats.  Uses and clears the scene's accumulator. */
-int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int passes, int64_t sample_offset, float* d_mean,
-                      float* d_var, nt_stats* stats);
+/* One pass of opts->samples_per_pixel (stratified, as nt_render; sample indices from sample_offset)
+ * with the radiance of every sample kept apart, then per pixel the mean radiance and the variance of
+ * that mean (sample variance / samples; 0 for one sample) into device arrays of pixel_count x 3
+ * floats.  The scene's accumulator is not touched. */
+int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int64_t sample_offset, float* d_mean, float* d_var,
+                      nt_stats* stats);
 
 /* Mean colour per pixel (pixel_count x 3 floats, x0 fastest) and the samples behind it. */
 int nt_accum_read(nt_scene* scene, float* rgb_mean, int64_t* samples_per_pixel);

@@ -145,6 +145,9 @@ struct PassDev
         long long sample_offset;  // first sample index of this pass (progressive passes)
         long long path_begin;     // first path of this launch window
         long long path_end;
+        int moments;              // 1: radiance is summed per path (index pixel * spp_eff + sample of
+                                  // the pass) instead of per pixel; the path queues then carry that
+                                  // index in place of the pixel
 };
 
 // Device-wide counters (one int64 each).

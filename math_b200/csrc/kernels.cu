@@ -255,7 +255,7 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevSce
         A.at(2 * N + 1, slot) = 1.0f;
         A.at(2 * N + 2, slot) = 1.0f;
         A.at(2 * N + 3, slot) = 1.0f;
-        A.pix[slot] = (uint32_t)pixel;
+        A.pix[slot] = P.moments ? (uint32_t)g : (uint32_t)pixel;
         A.smp[slot] = (uint32_t)sample;
         A.level[slot] = 0;
 }
@@ -490,7 +490,8 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                 float nr_org[N], nr_dir[N];
                 if (lit && level < S.max_depth)
                 {
-                        unsigned long long path = (unsigned long long)sample * (unsigned long long)P.npix + pixel;
+                        const unsigned long long px = P.moments ? pixel / (uint32_t)P.spp_eff : pixel;
+                        unsigned long long path = (unsigned long long)sample * (unsigned long long)P.npix + px;
                         float d[N];
                         if (cosine_hemisphere<N>(P.key0, P.key1, path, (uint32_t)(1 + level), sn, d))
                         {
@@ -875,31 +876,25 @@ __global__ void __launch_bounds__(BLOCK) k_aux(__grid_constant__ const DevScene<
         depth[i] = d;
 }
 
-// sum += v, sumsq += v^2 for the per-pixel values v of a single-sample pass
-__global__ void k_moments_add(long long n3, const double* __restrict__ accum, float* __restrict__ sum,
-                              float* __restrict__ sumsq)
+// Per-pixel mean and variance of the mean from per-path sums (path index pixel * spp + sample):
+// mean = sum / spp, var = (sum of squares - spp mean^2) / (spp - 1) / spp (0 for one sample).
+__global__ void k_moments_reduce(long long npix, int spp, const double* __restrict__ rad, float* __restrict__ mean,
+                                 float* __restrict__ var)
 {
-        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < npix * 3; i += (long long)gridDim.x * blockDim.x)
         {
-                const float v = (float)accum[i];
-                sum[i] += v;
-                sumsq[i] += v * v;
-        }
-}
-
-// sums of `passes` samples -> mean and the variance of the mean (sample variance / passes)
-__global__ void k_moments_finish(long long n3, int passes, float* __restrict__ mean, float* __restrict__ var)
-{
-        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
-        {
-                const float m = mean[i] / passes;
-                float v = 0;
-                if (passes > 1)
+                const long long p = i / 3;
+                const int c = (int)(i - p * 3);
+                double s1 = 0, s2 = 0;
+                for (int k = 0; k < spp; ++k)
                 {
-                        v = fmaxf(var[i] - passes * m * m, 0.0f) / (float)(passes - 1) / (float)passes;
+                        const double v = rad[((size_t)p * spp + k) * 3 + c];
+                        s1 += v;
+                        s2 += v * v;
                 }
-                mean[i] = m;
-                var[i] = v;
+                const double m = s1 / spp;
+                mean[i] = (float)m;
+                var[i] = spp > 1 ? (float)(fmax(s2 - spp * m * m, 0.0) / (spp - 1) / spp) : 0.0f;
         }
 }
 
@@ -1108,22 +1103,12 @@ cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, floa
         return cudaGetLastError();
 }
 
-cudaError_t launch_moments_add(long long n3, const double* accum, float* sum, float* sumsq, cudaStream_t st)
+cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, float* mean, float* var, cudaStream_t st)
 {
-        const unsigned g = (unsigned)std::min<long long>((n3 + BLOCK - 1) / BLOCK, 148LL * 32);
-        if (n3 > 0)
+        const unsigned g = (unsigned)std::min<long long>((npix * 3 + BLOCK - 1) / BLOCK, 148LL * 32);
+        if (npix > 0)
         {
-                k_moments_add<<<g, BLOCK, 0, st>>>(n3, accum, sum, sumsq);
-        }
-        return cudaGetLastError();
-}
-
-cudaError_t launch_moments_finish(long long n3, int passes, float* mean, float* var, cudaStream_t st)
-{
-        const unsigned g = (unsigned)std::min<long long>((n3 + BLOCK - 1) / BLOCK, 148LL * 32);
-        if (n3 > 0)
-        {
-                k_moments_finish<<<g, BLOCK, 0, st>>>(n3, passes, mean, var);
+                k_moments_reduce<<<g, BLOCK, 0, st>>>(npix, spp, rad, mean, var);
         }
         return cudaGetLastError();
 }

@@ -57,12 +57,11 @@ struct Wavefront
                         bool timing, const volatile int* stop);
 };
 
-// Denoiser inputs: first-hit normal and depth of every pixel-centre camera ray; moments of
-// single-sample passes.
+// Denoiser inputs: first-hit normal and depth of every pixel-centre camera ray; per-pixel mean and
+// variance of the mean from a pass rendered with per-path sums (PassDev::moments).
 template <int N>
 cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, float* depth, cudaStream_t st);
-cudaError_t launch_moments_add(long long n3, const double* accum, float* sum, float* sumsq, cudaStream_t st);
-cudaError_t launch_moments_finish(long long n3, int passes, float* mean, float* var, cudaStream_t st);
+cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, float* mean, float* var, cudaStream_t st);
 
 template <int N>
 cudaError_t launch_trace_closest(const MeshDev<N>& M, const float* org, const float* dir, long long nrays, int retest,

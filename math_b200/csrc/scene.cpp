@@ -318,6 +318,7 @@ struct nt_scene
         long long pool_paths = 0;
         int pool_lights = 0;
         DevBuf counters;
+        DevBuf moments;  // per-path sums of nt_render_moments
         unsigned long long* host_counters = nullptr;
         long long samples_done = 0;
         std::vector<unsigned char> dev_scene;  // packed DevScene<N>
@@ -1169,8 +1170,10 @@ int one_dimension_size(int n, int spp)
         return (int)std::ceil(v);
 }
 
+// One pass of samples_per_pixel; moments_accum: per-path sums (pixel * spp_eff + sample, 3 doubles
+// each, zeroed by the caller) instead of the scene's per-pixel accumulator (nt_render_moments).
 template <int N>
-void render(nt_scene* s, const nt_render_opts& o, nt_stats* st)
+void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_accum = nullptr)
 {
         auto t0 = std::chrono::steady_clock::now();
         if (o.samples_per_pixel < 1)
@@ -1222,10 +1225,15 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st)
         P.sample_offset = s->samples_done;
         P.path_begin = 0;
         P.path_end = total;
+        P.moments = moments_accum ? 1 : 0;
+        if (moments_accum && total > 0xffffffffll)
+        {
+                fail(NT_EINVAL, "too many paths in one moments pass");
+        }
         check_cuda(cudaMemsetAsync(s->counters.p, 0, s->counters.bytes, s->stream), "memset counters");
         KernelTimes times;
-        cudaError_t e = W.run(S, P, s->accum.as<double>(), s->counters.as<unsigned long long>(), s->host_counters, total,
-                              s->stream, &times, o.timing != 0, o.stop);
+        cudaError_t e = W.run(S, P, moments_accum ? moments_accum : s->accum.as<double>(), s->counters.as<unsigned long long>(),
+                              s->host_counters, total, s->stream, &times, o.timing != 0, o.stop);
         check_cuda(e, "render");
         check_cuda(cudaMemcpyAsync(s->host_counters, s->counters.p, C_COUNT * sizeof(unsigned long long),
                                    cudaMemcpyDeviceToHost, s->stream),
@@ -1433,6 +1441,14 @@ struct RenderF
         static void run(nt_scene* s, const nt_render_opts& o, nt_stats* st)
         {
                 render<N>(s, o, st);
+        }
+};
+template <int N>
+struct MomentsF
+{
+        static void run(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* acc)
+        {
+                render<N>(s, o, st, acc);
         }
 };
 template <int N>
@@ -1933,45 +1949,36 @@ int nt_render_aux(nt_scene* scene, float* d_normal, float* d_depth, void* stream
         });
 }
 
-int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int passes, int64_t sample_offset, float* d_mean,
-                      float* d_var, nt_stats* stats)
+int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int64_t sample_offset, float* d_mean, float* d_var,
+                      nt_stats* stats)
 {
         return guarded([&]() {
                 need_built(scene);
-                if (!opts || passes < 1 || sample_offset < 0 || !d_mean || !d_var)
+                if (!opts || sample_offset < 0 || !d_mean || !d_var)
                 {
                         fail(NT_EINVAL, "bad moments arguments");
                 }
-                const long long n3 = scene->pixel_count() * 3;
-                check_cuda(cudaMemsetAsync(d_mean, 0, n3 * sizeof(float), scene->stream), "memset");
-                check_cuda(cudaMemsetAsync(d_var, 0, n3 * sizeof(float), scene->stream), "memset");
-                nt_render_opts o = *opts;
-                o.samples_per_pixel = 1;
-                nt_stats total{};
-                for (int p = 0; p < passes; ++p)
+                const long long npix = scene->pixel_count();
+                const int spp = nt_effective_spp(scene->n, opts->samples_per_pixel);
+                if (spp < 1)
                 {
-                        check_cuda(cudaMemsetAsync(scene->accum.p, 0, scene->accum.bytes, scene->stream), "memset");
-                        scene->samples_done = sample_offset + p;
-                        nt_stats one{};
-                        dispatch<RenderF>(scene->n, scene, o, &one);
-                        check_cuda(launch_moments_add(n3, scene->accum.as<double>(), d_mean, d_var, scene->stream), "moments");
-                        total.paths += one.paths;
-                        total.rays += one.rays;
-                        total.shadow_rays += one.shadow_rays;
-                        total.facet_tests += one.facet_tests;
-                        total.box_steps += one.box_steps;
-                        total.retests += one.retests;
-                        total.descent_levels += one.descent_levels;
-                        total.error_bits |= one.error_bits;
-                        total.launches += one.launches + 1;
-                        total.seconds += one.seconds;
+                        fail(NT_EINVAL, "Stratified jittered sample count is not a positive integer");
                 }
-                check_cuda(launch_moments_finish(n3, passes, d_mean, d_var, scene->stream), "moments");
+                const size_t bytes = (size_t)npix * spp * 3 * sizeof(double);
+                if (scene->moments.bytes < bytes)
+                {
+                        scene->moments.alloc(bytes);
+                }
+                check_cuda(cudaMemsetAsync(scene->moments.p, 0, bytes, scene->stream), "memset");
+                scene->samples_done = sample_offset;
+                nt_stats one{};
+                dispatch<MomentsF>(scene->n, scene, *opts, &one, scene->moments.as<double>());
+                check_cuda(launch_moments_reduce(npix, spp, scene->moments.as<double>(), d_mean, d_var, scene->stream),
+                           "moments");
                 check_cuda(cudaStreamSynchronize(scene->stream), "moments sync");
-                total.spp_effective = passes;
                 if (stats)
                 {
-                        *stats = total;
+                        *stats = one;
                 }
         });
 }

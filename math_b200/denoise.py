@@ -202,21 +202,32 @@ def screen_axes(direction: np.ndarray) -> np.ndarray:
     return np.array(basis[1:], np.float32)
 
 
-def random_variant(n: int, rng: np.random.Generator, screen: int, extent: float = 8.0, max_tilt: float = 0.35) -> dict:
-    """Seeded light position, albedos in [0.3, 0.9] and a view direction tilted from -x_(n-1)."""
+def random_variant(n: int, rng: np.random.Generator, screen: int, extent: float = 8.0, max_tilt: float = 0.35,
+                   units_per_pixel: float | None = None) -> dict:
+    """Seeded light position, albedos in [0.3, 0.9] and a view direction tilted from -x_(n-1).  With
+    units_per_pixel the screen is a window of that pixel scale at a seeded place inside the
+    extent x ... x extent view (training crops at the scale of a larger evaluation screen)."""
     light = np.concatenate([rng.uniform(-3.0, 3.0, n - 1), rng.uniform(2.0, 4.0, 1)]).astype(np.float32)
     tilt = rng.normal(size=n - 1)
     tilt *= rng.uniform(0.0, max_tilt) / max(np.linalg.norm(tilt), 1e-9)
     d = np.concatenate([tilt, [-1.0]])
     d /= np.linalg.norm(d)
+    d = d.astype(np.float32)
+    org = -10.0 * d.astype(np.float64)
+    upp = extent / screen
+    if units_per_pixel is not None:
+        upp = float(units_per_pixel)
+        half = max(0.0, 0.5 * (extent - screen * upp))
+        axes = screen_axes(d).astype(np.float64)
+        org = org + (rng.uniform(-half, half, n - 1) @ axes)
     return {
         "light": light,
         "mesh_albedo": float(rng.uniform(0.3, 0.9)),
         "floor_albedo": float(rng.uniform(0.3, 0.9)),
-        "dir": d.astype(np.float32),
-        "org": (-10.0 * d).astype(np.float32),
+        "dir": d,
+        "org": org.astype(np.float32),
         "screen": [screen] * (n - 1),
-        "param": extent / screen,
+        "param": upp,
     }
 
 
@@ -234,8 +245,9 @@ def apply_variant(scene: ntrace.Scene, v: dict, has_floor: bool = True) -> None:
     scene.build()
 
 
-def render_inputs(scene: ntrace.Scene, passes: int, seed: int, max_depth: int = 5, sample_offset: int = 0) -> dict:
-    """Noisy input of the denoiser: `passes` single-sample passes plus the first-hit features."""
+def render_inputs(scene: ntrace.Scene, spp: int, seed: int, max_depth: int = 5, sample_offset: int = 0) -> dict:
+    """Noisy input of the denoiser: one pass of spp samples per pixel (per-pixel mean and variance of
+    the mean) plus the first-hit normal and depth."""
     import torch
 
     P, n = scene.pixel_count, scene.n
@@ -246,7 +258,7 @@ def render_inputs(scene: ntrace.Scene, passes: int, seed: int, max_depth: int = 
         "depth": torch.empty((P,), dtype=torch.float32, device="cuda"),
     }
     torch.cuda.synchronize()
-    scene.render_moments(passes, out["mean"].data_ptr(), out["var"].data_ptr(), sample_offset=sample_offset,
+    scene.render_moments(spp, out["mean"].data_ptr(), out["var"].data_ptr(), sample_offset=sample_offset,
                          max_depth=max_depth, seed=seed)
     scene.render_aux(out["normal"].data_ptr(), out["depth"].data_ptr())
     return out
@@ -263,17 +275,16 @@ def render_reference(scene: ntrace.Scene, spp: int, seed: int, max_depth: int = 
 
 
 def make_pairs(scene: ntrace.Scene, count: int, seed: int, screen: int, spp_in: int, spp_ref: int,
-               max_depth: int = 5, has_floor: bool = True) -> list[dict]:
-    """`count` training pairs from seeded variations of `scene`: spp_in samples per pixel as single-
-    sample passes (the noisy input with its moments) and spp_ref stratified samples (the target)."""
+               max_depth: int = 5, has_floor: bool = True, units_per_pixel: float | None = None) -> list[dict]:
+    """`count` training pairs from seeded variations of `scene`: spp_in samples per pixel (the noisy
+    input with its moments) and spp_ref samples (the target), both stratified."""
     n = scene.n
     rng = np.random.default_rng(seed)
-    passes = ntrace.effective_spp(n, spp_in)
     pairs = []
     for i in range(count):
-        v = random_variant(n, rng, screen)
+        v = random_variant(n, rng, screen, units_per_pixel=units_per_pixel)
         apply_variant(scene, v, has_floor)
-        x = render_inputs(scene, passes, seed=seed * 100003 + 2 * i, max_depth=max_depth)
+        x = render_inputs(scene, spp_in, seed=seed * 100003 + 2 * i, max_depth=max_depth)
         x["target"] = render_reference(scene, spp_ref, seed=seed * 100003 + 2 * i + 1, max_depth=max_depth)
         x["screen"] = list(v["screen"])
         pairs.append(x)

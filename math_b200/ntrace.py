@@ -133,8 +133,7 @@ def library() -> ctypes.CDLL:
         "nt_scene_clear_lights": ([vp], ctypes.c_int),
         "nt_scene_set_object_surface": ([vp, ctypes.c_int, ctypes.POINTER(Surface)], ctypes.c_int),
         "nt_render_aux": ([vp, vp, vp, vp], ctypes.c_int),
-        "nt_render_moments": ([vp, ctypes.POINTER(RenderOpts), ctypes.c_int, i64, vp, vp, ctypes.POINTER(Stats)],
-                              ctypes.c_int),
+        "nt_render_moments": ([vp, ctypes.POINTER(RenderOpts), i64, vp, vp, ctypes.POINTER(Stats)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -319,13 +318,13 @@ class Scene:
         """First-hit normal (pixels x n) and depth (pixels) into device arrays (pointers as integers)."""
         _check(self._lib.nt_render_aux(self._h, d_normal, d_depth, stream or None))
 
-    def render_moments(self, passes: int, d_mean: int, d_var: int, sample_offset: int = 0, max_depth: int = 100,
-                       seed: int = 0, retest: bool = True) -> dict:
-        """`passes` single-sample passes: per-pixel mean and variance of the mean into device arrays."""
-        o = RenderOpts(1, int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)), 0, 0, 0, None)
+    def render_moments(self, samples_per_pixel: int, d_mean: int, d_var: int, sample_offset: int = 0,
+                       max_depth: int = 100, seed: int = 0, retest: bool = True) -> dict:
+        """One pass of samples_per_pixel: per-pixel mean and variance of the mean into device arrays."""
+        o = RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)), 0, 0, 0,
+                       None)
         st = Stats()
-        _check(self._lib.nt_render_moments(self._h, ctypes.byref(o), int(passes), int(sample_offset), d_mean, d_var,
-                                           ctypes.byref(st)))
+        _check(self._lib.nt_render_moments(self._h, ctypes.byref(o), int(sample_offset), d_mean, d_var, ctypes.byref(st)))
         return st.as_dict()
 
     def trace_closest(self, org, dirs, mesh_index: int = 0, retest: bool = True):

@@ -1,0 +1,165 @@
+"""Trains the learned denoiser (one network per dimension) on pairs rendered by the tracer, and
+measures the time to a relative RMSE of 1e-2 against a 64k-sample render, plain versus denoised.
+
+    python -m math_b200.train_denoiser --n 3 4 5 --pairs 200 --steps 3000 --out math_b200/weights
+
+Training pairs: seeded variations (light position, view direction, albedos in [0.3, 0.9]) of the
+measured scenes' meshes on small screens; the noisy input is a few samples per pixel (its per-pixel
+mean and variance of the mean), plus the first-hit normal and depth; the target is a 4096-sample
+render.  The input sample count of each pair is drawn from --spp-in, so one
+network covers several noise levels.  Weights go to <out>/denoiser_n<n>.npz.
+
+Evaluation (--eval): a held-out variation on a larger screen; the reference is a 64k-sample render
+(effective k^(n-1) >= 65536); plain renders at 1, 4, 16, ... samples and denoised renders of the
+inputs at each --spp-in give (time, relative RMSE) points; the report is the time each method needs
+to reach --target (the smallest measured spp that reaches it).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+from . import denoise, ntrace, scenes
+
+TRAIN_SCREEN = {3: 64, 4: 24, 5: 10, 6: 6}   # training crops, at the evaluation screen's pixel scale
+EVAL_SCREEN = {3: 256, 4: 48, 5: 16, 6: 8}    # evaluation: the whole 8 x ... x 8 view
+EXTENT = 8.0
+REF_SPP = 65536
+
+
+def mesh_for(n: int, small: bool = False):
+    """The measured scene's mesh (or the reduced test mesh)."""
+    if small:
+        return scenes.config(f"n{n}_small")
+    if n == 3:
+        v, f = scenes.icosphere(5)
+        return scenes.make_spec(3, v, f, screen=TRAIN_SCREEN[3], spp=4)
+    if n == 4:
+        v, f = scenes.sphere_hull(4, 100_000, seed=0)
+        return scenes.make_spec(4, v, f, screen=TRAIN_SCREEN[4], spp=4)
+    if n == 5:
+        v, f = scenes.sphere_hull(5, 50_000, seed=0, cap=0.5)
+        return scenes.make_spec(5, v, f, screen=TRAIN_SCREEN[5], spp=4)
+    v, f = scenes.sphere_hull(6, 5_000, seed=0)
+    return scenes.make_spec(6, v, f, screen=TRAIN_SCREEN[6], spp=4)
+
+
+def make_mixed_pairs(scene, n: int, count: int, seed: int, spp_in: list[int], spp_ref: int) -> list[dict]:
+    pairs = []
+    rng = np.random.default_rng(seed)
+    for i in range(count):
+        s = int(spp_in[rng.integers(len(spp_in))])
+        pairs += denoise.make_pairs(scene, 1, seed=seed * 7919 + i, screen=TRAIN_SCREEN[n], spp_in=s, spp_ref=spp_ref,
+                                    units_per_pixel=EXTENT / EVAL_SCREEN[n])
+    return pairs
+
+
+def time_to_rmse(scene, den, n: int, screen: int, spp_in: list[int], target: float, seed: int,
+                 max_plain_spp: int = 1 << 14) -> dict:
+    """(time, RMSE) of plain and denoised renders of one held-out variation against a 64k render."""
+    import torch
+
+    rng = np.random.default_rng(seed)
+    v = denoise.random_variant(n, rng, screen)
+    denoise.apply_variant(scene, v)
+    t0 = time.perf_counter()
+    ref = denoise.render_reference(scene, REF_SPP, seed=seed + 1)
+    ref_s = time.perf_counter() - t0
+    plain = []
+    spp = 1
+    while spp <= max_plain_spp:
+        scene.clear()
+        t0 = time.perf_counter()
+        scene.render(spp, max_depth=5, seed=seed + 2 + spp)
+        dt = time.perf_counter() - t0
+        img, _ = scene.image()
+        plain.append({"spp": ntrace.effective_spp(n, spp), "seconds": dt, "rmse": denoise.relative_rmse(img, ref)})
+        if plain[-1]["rmse"] <= target:
+            break
+        spp *= 4
+    den_pts = []
+    for s in spp_in:
+        # warm (allocations of the denoiser's workspace happen on first use)
+        x = denoise.render_inputs(scene, s, seed=seed + 5)
+        den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
+        den.apply()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x = denoise.render_inputs(scene, s, seed=seed + 7)
+        den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
+        out = den.apply()
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        den_pts.append({"spp": ntrace.effective_spp(n, s), "seconds": dt, "rmse": denoise.relative_rmse(out, ref),
+                        "input_rmse": denoise.relative_rmse(x["mean"], ref)})
+
+    def first(points):
+        ok = [p for p in points if p["rmse"] <= target]
+        return min(ok, key=lambda p: p["seconds"]) if ok else None
+
+    bp, bd = first(plain), first(den_pts)
+    return {"n": n, "screen": [screen] * (n - 1), "reference_spp": ntrace.effective_spp(n, REF_SPP),
+            "reference_seconds": ref_s, "target_rmse": target, "plain": plain, "denoised": den_pts,
+            "plain_time_to_target": bp["seconds"] if bp else None,
+            "denoised_time_to_target": bd["seconds"] if bd else None,
+            "speedup": (bp["seconds"] / bd["seconds"]) if (bp and bd) else None}
+
+
+def main(argv=None) -> None:
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--n", type=int, nargs="+", default=[3, 4, 5])
+    ap.add_argument("--pairs", type=int, default=200)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--spp-in", type=int, nargs="+", default=[4, 16, 64])
+    ap.add_argument("--spp-ref", type=int, default=4096)
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--out", default=str(Path(__file__).resolve().parent / "weights"))
+    ap.add_argument("--small", action="store_true", help="reduced test meshes instead of the measured ones")
+    ap.add_argument("--eval", action="store_true")
+    ap.add_argument("--target", type=float, default=1e-2)
+    ap.add_argument("--load", action="store_true", help="evaluate saved weights instead of training")
+    args = ap.parse_args(argv)
+    out = Path(args.out)
+    out.mkdir(parents=True, exist_ok=True)
+    for n in args.n:
+        t0 = time.perf_counter()
+        spec = mesh_for(n, args.small)
+        scene = scenes.build_scene(spec)
+        build_s = time.perf_counter() - t0
+        path = out / f"denoiser_n{n}.npz"
+        report = {"n": n, "scene_build_seconds": build_s}
+        if args.load:
+            den = denoise.Denoiser.load(path)
+        else:
+            t0 = time.perf_counter()
+            pairs = make_mixed_pairs(scene, n, args.pairs, args.seed + n, args.spp_in, args.spp_ref)
+            report["pairs_seconds"] = time.perf_counter() - t0
+            held = make_mixed_pairs(scene, n, max(4, args.pairs // 10), args.seed + 1000 + n, args.spp_in,
+                                    args.spp_ref)
+            den = denoise.Denoiser(n, seed=args.seed)
+            uni = denoise.Denoiser(n, seed=args.seed)
+            uni.set_params(denoise.uniform_filter_params(uni))
+            t0 = time.perf_counter()
+            losses = denoise.train(den, pairs, args.steps, args.lr, seed=args.seed)
+            report["train_seconds"] = time.perf_counter() - t0
+            report["loss_first_100"] = float(np.mean(losses[:100]))
+            report["loss_last_100"] = float(np.mean(losses[-100:]))
+            report["held_out"] = {"trained": denoise.evaluate(den, held), "uniform": denoise.evaluate(uni, held)}
+            den.save(path)
+            report["weights"] = str(path)
+        if args.eval:
+            report["time_to_rmse"] = time_to_rmse(scene, den, n, EVAL_SCREEN[n], args.spp_in, args.target,
+                                                  seed=args.seed + 77 + n)
+        print(json.dumps(report), flush=True)
+        scene.close()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -159,11 +159,10 @@ def test_moments_and_first_hit_inputs(require_gpu):
     v, f = scenes.icosphere(2)
     spec = scenes.make_spec(3, v, f, screen=24, spp=4, max_depth=3, seed=0)
     scene = scenes.build_scene(spec)
-    x = denoise.render_inputs(scene, passes=4, seed=11, max_depth=3)
-    # the same four single-sample passes through the ordinary render give the same mean
+    x = denoise.render_inputs(scene, 4, seed=11, max_depth=3)
+    # the same pass through the ordinary render (same samples, summed per pixel) gives the same mean
     scene.clear()
-    for _ in range(4):
-        scene.render(1, max_depth=3, seed=11)
+    scene.render(4, max_depth=3, seed=11)
     plain, spp = scene.image()
     assert spp == 4
     np.testing.assert_allclose(x["mean"].cpu().numpy(), plain, rtol=1e-5, atol=1e-6)
