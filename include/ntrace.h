@@ -121,6 +121,15 @@ int nt_scene_destroy(nt_scene* scene);
 int nt_scene_add_mesh(nt_scene* scene, const float* vertices, int64_t vertex_count, const int32_t* facets,
                       int64_t facet_count, const nt_surface* surface);
 
+/* Vertex normals of mesh object `object` (the Obj's normals and per-facet normal indices that
+ * MeshHyperplaneSimplex takes, mesh_hyperplane_simplex.cpp:59-143): normals is normal_count x n;
+ * facet_normals is facet_count x n indices into normals, or NULL for the facet's vertex indices.  Each
+ * facet is classified as the reference does: any |cos(vertex normal, facet normal)| < 0.7 -> flat;
+ * all positive -> interpolated; all negative -> interpolated with the facet normal reversed; mixed ->
+ * interpolated with the negative ones reversed.  Used when nt_render_opts.smooth_normal is set. */
+int nt_scene_set_mesh_normals(nt_scene* scene, int object, const float* normals, int64_t normal_count,
+                              const int32_t* facet_normals);
+
 /* n-parallelotope: VisibleParallelotope(org, e0..e(n-1)) (visible_shapes.h:75-117).  edges: n x n. */
 int nt_scene_add_parallelotope(nt_scene* scene, const float* org, const float* edges, const nt_surface* surface);
 

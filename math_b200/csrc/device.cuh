@@ -1684,6 +1684,57 @@ __device__ __forceinline__ void closest_finish(const ClosestPlan& p, bool hit, f
 }
 
 // ------------------------------------------------------------------------------------------------
+// Shading normal of a mesh facet with vertex normals (MeshHyperplaneSimplex::shading_normal,
+// mesh_hyperplane_simplex.cpp:157-186): the vertex normals (reversed where the facet's type says so)
+// interpolated with the barycentric coordinates of the point (HyperplaneSimplexGeometry::
+// barycentric_coordinates / interpolate, hyperplane_geometry.h:169-219), normalised.  Returns false
+// for a flat facet (NormalType::None: the shading normal is the geometric one).
+
+template <int N>
+__device__ __forceinline__ bool smooth_normal(const MeshDev<N>& M, int facet, const float* p, float* sn)
+{
+        const int type = M.ntype[facet];
+        if ((type & 3) == 0)
+        {
+                return false;
+        }
+        const float4* rec = M.rec32 + (size_t)facet * Rec32<N>::F4;
+        float f[Rec32<N>::FLOATS];
+#pragma unroll
+        for (int q = 0; q < Rec32<N>::F4; ++q)
+        {
+                float4 v = __ldg(rec + q);
+                f[4 * q + 0] = v.x;
+                f[4 * q + 1] = v.y;
+                f[4 * q + 2] = v.z;
+                f[4 * q + 3] = v.w;
+        }
+        float bc[N];
+        bc[N - 1] = 1.0f;
+#pragma unroll
+        for (int i = 0; i < N - 1; ++i)
+        {
+                const float* pl = f + Rec32<N>::OFF_PLANES + i * (N + 1);
+                bc[i] = vdot<N>(p, pl) - pl[N];
+                bc[N - 1] -= bc[i];
+        }
+#pragma unroll
+        for (int i = 0; i < N; ++i)
+        {
+                const float* vn = M.vnormals + (size_t)__ldg(&M.fnormals[(size_t)facet * N + i]) * N;
+                const bool rev = (type & 3) == 2 && (type & (1 << (2 + i)));
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        const float c = rev ? -__ldg(vn + k) : __ldg(vn + k);
+                        sn[k] = (i == 0) ? bc[0] * c : sn[k] + bc[i] * c;
+                }
+        }
+        vnormalize<N>(sn);
+        return true;
+}
+
+// ------------------------------------------------------------------------------------------------
 // Sampling (sphere.h:87-116, complement.h:71-200)
 
 template <int N>

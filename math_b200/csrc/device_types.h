@@ -56,6 +56,12 @@ struct MeshDev
         const double* rec64;
         const int2* nodes;     // internal: {first_child, -1}; leaf: {index offset, count}
         const int* leaf_idx;
+        // vertex normals (null without them): normals (count x N), per-facet normal indices (N per
+        // facet) and per-facet NormalType: 0 None, 1 Use, 2 Reverse with bit 2 + i set when vertex i's
+        // normal is reversed (mesh_hyperplane_simplex.cpp:96-143)
+        const float* vnormals;
+        const int* fnormals;
+        const int* ntype;
         int nfacets;
         int levels;
         float root_org[N];
@@ -170,6 +176,7 @@ enum Counter : int
         // work cursors of the persistent extension and shadow kernels
         C_WORK_EXT = 13,
         C_WORK_SH = 14,
+        C_SMOOTH = 15,  // entries of the smooth-normal shadow queue
         C_COUNT = 16
 };
 

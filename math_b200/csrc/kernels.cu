@@ -322,8 +322,8 @@ __device__ __forceinline__ void accumulate(double* accum, uint32_t pixel, float 
 // the shadow queue and, below the depth cap, writes its continuation into the next path queue.
 template <int N>
 __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, HitView<N> H,
-                                                 PathView<N> B, ShadowView<N> SQ, double* accum, long long count,
-                                                 unsigned long long* counters)
+                                                 PathView<N> B, ShadowView<N> SQ, ShadowView<N> SM, double* accum,
+                                                 long long count, unsigned long long* counters)
 {
         __shared__ int s_warp[BLOCK / 32];
         __shared__ long long s_base;
@@ -337,6 +337,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                 float ncl = 0;
                 float p[N], gn[N], sn[N];
                 bool mesh = false;
+                bool smooth = false;  // sn holds the interpolated vertex normal (before the flip)
                 uint32_t pixel = 0, sample = 0;
                 int level = 0;
                 int err = 0;
@@ -369,7 +370,9 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                 const ObjDev& ob = S.obj[obj];
                                 if (ob.kind == OBJ_MESH)
                                 {
-                                        const float4* rec = S.mesh[ob.index].rec32 + (size_t)H.facet[i] * Rec32<N>::F4;
+                                        const MeshDev<N>& MM = S.mesh[ob.index];
+                                        const int facet = H.facet[i];
+                                        const float4* rec = MM.rec32 + (size_t)facet * Rec32<N>::F4;
                                         float f4[(N + 3) / 4 * 4];
 #pragma unroll
                                         for (int q = 0; q < (N + 3) / 4; ++q)
@@ -384,6 +387,10 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                         for (int k = 0; k < N; ++k)
                                         {
                                                 gn[k] = f4[k];
+                                        }
+                                        if (S.smooth_normal && MM.ntype)
+                                        {
+                                                smooth = smooth_normal<N>(MM, facet, p, sn);
                                         }
                                 }
                                 else if (ob.kind == OBJ_PLT)
@@ -410,18 +417,24 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                         }
                                         else
                                         {
+                                                // only the geometric normal decides the side; the shading
+                                                // normal turns with it (painter.cpp:369-373)
                                                 if (dd > 0)
                                                 {
 #pragma unroll
                                                         for (int k = 0; k < N; ++k)
                                                         {
                                                                 gn[k] = -gn[k];
+                                                                sn[k] = -sn[k];
                                                         }
                                                 }
-#pragma unroll
-                                                for (int k = 0; k < N; ++k)
+                                                if (!smooth)
                                                 {
-                                                        sn[k] = gn[k];
+#pragma unroll
+                                                        for (int k = 0; k < N; ++k)
+                                                        {
+                                                                sn[k] = gn[k];
+                                                        }
                                                 }
                                                 if (ob.diffuse > 0)
                                                 {
@@ -440,6 +453,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                 for (int l = 0; l < S.nlights; ++l)
                 {
                         bool shadow = false;
+                        bool behind = false;  // smooth-normal branch (painter.cpp:238-284)
                         float sh_org[N], sh_dir[N], sh_tmax = 0, sh_c[3] = {0, 0, 0};
                         if (lit)
                         {
@@ -452,9 +466,12 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                         float dln = vdot<N>(lr.dir, sn);
                                         if (dln > 0)
                                         {
+                                                // a smooth-shaded mesh point whose geometric side faces away
+                                                // from the light takes the smooth-normal branch
+                                                behind = mesh && S.smooth_normal && vdot<N>(lr.dir, gn) < 0;
                                                 ray_move<N>(lr, S.ray_offset);
                                                 float w = S.diffuse_coef * dln;
-                                                shadow = true;
+                                                shadow = !behind;
 #pragma unroll
                                                 for (int k = 0; k < N; ++k)
                                                 {
@@ -482,6 +499,25 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                 SQ.at(2 * N + 2, qo) = sh_c[1];
                                 SQ.at(2 * N + 3, qo) = sh_c[2];
                                 SQ.pix[qo] = pixel;
+                        }
+                        if (S.smooth_normal)
+                        {
+                                // block-uniform: every thread of the block takes part in the compaction
+                                long long bo = compact_slot(behind, counters + C_SMOOTH, s_warp, &s_base);
+                                if (behind)
+                                {
+#pragma unroll
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                SM.at(k, bo) = sh_org[k];
+                                                SM.at(N + k, bo) = sh_dir[k];
+                                        }
+                                        SM.at(2 * N + 0, bo) = sh_tmax;
+                                        SM.at(2 * N + 1, bo) = sh_c[0];
+                                        SM.at(2 * N + 2, bo) = sh_c[1];
+                                        SM.at(2 * N + 3, bo) = sh_c[2];
+                                        SM.pix[bo] = pixel;
+                                }
                         }
                 }
 
@@ -563,6 +599,58 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_consta
                                 accumulate(accum, SQ.pix[i], SQ.at(2 * N + 1, i), SQ.at(2 * N + 2, i), SQ.at(2 * N + 3, i));
                         }
                         ++rays;
+                }
+        }
+        flush_stats<true>(counters, ws, 0, rays);
+}
+
+// The smooth-normal branch of direct_diffuse_lighting (painter.cpp:238-284): a smooth-shaded mesh
+// point whose geometric side faces away from the light.  The ray to the light (already moved by the
+// ray offset) must hit something before the light; the reverse ray must not hit anything nearer than
+// that; the light is then tested from just beyond that first hit.  Rare (only meshes with vertex
+// normals, only with smooth_normal), so one ray per thread through the general scene functions.
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_shadow_smooth(__grid_constant__ const DevScene<N> S, ShadowView<N> SM,
+                                                         double* accum, long long count, unsigned long long* counters)
+{
+        WalkStats ws{0, 0, 0, 0, 0};
+        long long rays = 0;
+        const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+        if (i < count)
+        {
+                Ray<N> r;
+#pragma unroll
+                for (int k = 0; k < N; ++k)
+                {
+                        r.org[k] = SM.at(k, i);
+                        r.dir[k] = SM.at(N + k, i);
+                }
+                const float dist = SM.at(2 * N, i);
+                float t, t_rev;
+                int obj, facet;
+                rays = 1;
+                bool lit = false;
+                if (scene_closest<N>(S, r, &t, &obj, &facet, &ws) && t < dist)
+                {
+                        Ray<N> rev;
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                rev.org[k] = r.org[k];
+                                rev.dir[k] = -r.dir[k];
+                        }
+                        ray_move<N>(rev, 2 * S.ray_offset);
+                        rays = 2;
+                        if (!(scene_closest<N>(S, rev, &t_rev, &obj, &facet, &ws) && t_rev < t))
+                        {
+                                ray_move<N>(r, t + S.ray_offset);
+                                rays = 3;
+                                lit = scene_visible<N>(S, r, dist - t, &ws);
+                        }
+                }
+                if (lit)
+                {
+                        accumulate(accum, SM.pix[i], SM.at(2 * N + 1, i), SM.at(2 * N + 2, i), SM.at(2 * N + 3, i));
                 }
         }
         flush_stats<true>(counters, ws, 0, rays);
@@ -921,17 +1009,17 @@ long long resident_blocks(K kernel)
 // Host-side launchers
 
 template <int N>
-size_t Wavefront<N>::bytes_for(long long Q, int lights)
+size_t Wavefront<N>::bytes_for(long long Q, int lights, bool smooth)
 {
         size_t per_path = sizeof(float) * (2 * N + 4) * 2  // path state A and B
                           + sizeof(uint32_t) * 2 * 2 + sizeof(int) * 2
                           + sizeof(float) + sizeof(int) * 2  // hit record
-                          + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights;  // shadow queue
-        return per_path * (size_t)Q + 16 * 256;
+                          + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights * (smooth ? 2 : 1);  // shadow queues
+        return per_path * (size_t)Q + 18 * 256;
 }
 
 template <int N>
-void Wavefront<N>::carve(char* base, long long Q, int lights)
+void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
 {
         this->Q = Q;
         this->lights = lights;
@@ -953,6 +1041,16 @@ void Wavefront<N>::carve(char* base, long long Q, int lights)
         hit_facet = (int*)take(sizeof(int) * Q);
         sq_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
         sq_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
+        if (smooth)
+        {
+                sm_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
+                sm_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
+        }
+        else
+        {
+                sm_f = nullptr;
+                sm_pix = nullptr;
+        }
 }
 
 template <int N>
@@ -990,6 +1088,7 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                 PathView<N> B{fb, flip ? pixA : pixB, flip ? smpA : smpB, flip ? lvlA : lvlB, Q};
                 HitView<N> H{hit_t, hit_obj, hit_facet};
                 ShadowView<N> SQ{sq_f, sq_pix, Q * lights};
+                ShadowView<N> SM{sm_f, sm_pix, Q * lights};
 
                 long long fresh = std::min(Q - active, total_paths - next);
                 if (timing)
@@ -1024,13 +1123,18 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                         cudaEventRecord(ev[2], st);
                 }
                 cudaMemsetAsync(counters + C_ACTIVE_OUT, 0, 2 * sizeof(unsigned long long), st);
+                cudaMemsetAsync(counters + C_SMOOTH, 0, sizeof(unsigned long long), st);
                 long long shade_blocks = std::min<long long>(grid_for<N>(active), 148LL * 16);
-                k_shade<N><<<(unsigned)shade_blocks, BLOCK, 0, st>>>(S, P, A, H, B, SQ, accum, active, counters);
+                if (S.smooth_normal && !sm_f)
+                {
+                        return cudaErrorInvalidValue;  // the pool was carved without the smooth-normal queue
+                }
+                k_shade<N><<<(unsigned)shade_blocks, BLOCK, 0, st>>>(S, P, A, H, B, SQ, SM, accum, active, counters);
                 if (timing)
                 {
                         cudaEventRecord(ev[3], st);
                 }
-                cudaMemcpyAsync(host_counters, counters, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+                cudaMemcpyAsync(host_counters, counters, C_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
                 cudaError_t e = cudaStreamSynchronize(st);
                 if (e != cudaSuccess)
                 {
@@ -1038,6 +1142,13 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                 }
                 long long survivors = (long long)host_counters[C_ACTIVE_OUT];
                 long long shadows = (long long)host_counters[C_SHADOW];
+                long long smooth_rays = (long long)host_counters[C_SMOOTH];
+                if (smooth_rays > 0)
+                {
+                        k_shadow_smooth<N><<<(unsigned)grid_for<N>(smooth_rays), BLOCK, 0, st>>>(S, SM, accum, smooth_rays,
+                                                                                                   counters);
+                        times->launches += 1;
+                }
                 if (shadows > 0 && one_mesh)
                 {
                         k_shadow_refill<N><<<(unsigned)std::min(shadow_refill_blocks, grid_for<N>(shadows)), BLOCK, 0, st>>>(

@@ -44,9 +44,12 @@ struct Wavefront
         int* hit_facet = nullptr;
         float* sq_f = nullptr;
         uint32_t* sq_pix = nullptr;
+        // smooth-normal shadow queue (only when some mesh has vertex normals and smooth_normal is set)
+        float* sm_f = nullptr;
+        uint32_t* sm_pix = nullptr;
 
-        static size_t bytes_for(long long Q, int lights);
-        void carve(char* base, long long Q, int lights);
+        static size_t bytes_for(long long Q, int lights, bool smooth = false);
+        void carve(char* base, long long Q, int lights, bool smooth = false);
 
         // Traces total_paths camera paths starting at P.path_begin into accum (3 doubles per pixel).
         // counters: C_COUNT device int64; host_counters: pinned host mirror of the first two.

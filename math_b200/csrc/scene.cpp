@@ -220,6 +220,8 @@ struct MeshHost
         std::vector<float> vertices;
         std::vector<int32_t> facets;
         nt_surface surface;
+        std::vector<float> normals;           // vertex normals (optional)
+        std::vector<int32_t> facet_normals;   // N normal indices per facet
         // built
         std::vector<float> rec32;
         std::vector<double> rec64;
@@ -232,7 +234,9 @@ struct MeshHost
         long long leaf_count = 0;
         long long degenerate = 0;
         double build_seconds = 0;
+        std::vector<int32_t> ntype;  // per facet: NormalType and reversed-vertex bits (MeshDev::ntype)
         DevBuf d_rec32, d_rec64, d_nodes, d_idx;
+        DevBuf d_normals, d_fnormals, d_ntype;
         // pinned host copy of the four device arrays, back to back (re-upload, nt_scene_upload)
         void* pinned = nullptr;
         size_t pinned_bytes = 0;
@@ -245,12 +249,15 @@ struct MeshHost
         MeshHost(const MeshHost&) = delete;
         MeshHost& operator=(const MeshHost&) = delete;
         MeshHost(MeshHost&& o) noexcept
-                : vertices(std::move(o.vertices)), facets(std::move(o.facets)), surface(o.surface), rec32(std::move(o.rec32)),
+                : vertices(std::move(o.vertices)), facets(std::move(o.facets)), surface(o.surface),
+                  normals(std::move(o.normals)), facet_normals(std::move(o.facet_normals)), rec32(std::move(o.rec32)),
                   rec64(std::move(o.rec64)), nodes(std::move(o.nodes)), leaf_idx(std::move(o.leaf_idx)),
                   level_sizes(std::move(o.level_sizes)), root_org(std::move(o.root_org)), root_d1(std::move(o.root_d1)),
                   dist(o.dist), vmin(std::move(o.vmin)), vmax(std::move(o.vmax)), leaf_count(o.leaf_count),
-                  degenerate(o.degenerate), build_seconds(o.build_seconds), d_rec32(std::move(o.d_rec32)),
-                  d_rec64(std::move(o.d_rec64)), d_nodes(std::move(o.d_nodes)), d_idx(std::move(o.d_idx)),
+                  degenerate(o.degenerate), build_seconds(o.build_seconds), ntype(std::move(o.ntype)),
+                  d_rec32(std::move(o.d_rec32)), d_rec64(std::move(o.d_rec64)), d_nodes(std::move(o.d_nodes)),
+                  d_idx(std::move(o.d_idx)), d_normals(std::move(o.d_normals)), d_fnormals(std::move(o.d_fnormals)),
+                  d_ntype(std::move(o.d_ntype)),
                   pinned(o.pinned), pinned_bytes(o.pinned_bytes), ready(o.ready), uploaded(o.uploaded)
         {
                 o.pinned = nullptr;
@@ -317,6 +324,7 @@ struct nt_scene
         DevBuf pool;
         long long pool_paths = 0;
         int pool_lights = 0;
+        bool pool_smooth = false;
         DevBuf counters;
         DevBuf moments;  // per-path sums of nt_render_moments
         unsigned long long* host_counters = nullptr;
@@ -385,6 +393,15 @@ void build_mesh(MeshHost& m, unsigned threads)
         m.rec64.assign((size_t)nf * Rec64<N>::DOUBLES, 0.0);
         std::atomic<long long> degenerate{0};
         std::atomic<long long> bad{-1};
+        const bool has_normals = !m.normals.empty();
+        if (has_normals)
+        {
+                m.ntype.assign(nf, 0);
+        }
+        else
+        {
+                m.ntype.clear();
+        }
         parallel_for((nf + 1023) / 1024, threads, [&](long long chunk) {
                 long long end = std::min(nf, (chunk + 1) * 1024);
                 for (long long f = chunk * 1024; f < end; ++f)
@@ -478,6 +495,56 @@ void build_mesh(MeshHost& m, unsigned threads)
                         }
                         r32[Rec32<N>::OFF_B] = B;
                         r32[Rec32<N>::OFF_D] = D;
+                        if (has_normals)
+                        {
+                                // NormalType (mesh_hyperplane_simplex.cpp:96-143); LIMIT_COSINE = 0.7
+                                double dots[N];
+                                bool flat = false, all_pos = true, all_neg = true;
+                                for (int i = 0; i < N; ++i)
+                                {
+                                        const float* vn = &m.normals[(size_t)m.facet_normals[f * N + i] * N];
+                                        double d = 0;
+                                        for (int k = 0; k < N; ++k)
+                                        {
+                                                d += (double)vn[k] * n64[k];
+                                        }
+                                        dots[i] = d;
+                                        flat |= std::fabs(d) < 0.7;
+                                        all_pos &= d > 0;
+                                        all_neg &= d < 0;
+                                }
+                                int type = 0;
+                                if (!flat && all_pos)
+                                {
+                                        type = 1;
+                                }
+                                else if (!flat && all_neg)
+                                {
+                                        // the facet normal is reversed to agree with the vertex normals (the
+                                        // intersection distance does not depend on its sign)
+                                        type = 1;
+                                        for (int k = 0; k <= N; ++k)
+                                        {
+                                                if (k < N)
+                                                {
+                                                        r64[Rec64<N>::OFF_NORMAL + k] = -r64[Rec64<N>::OFF_NORMAL + k];
+                                                }
+                                                r32[k] = -r32[k];
+                                        }
+                                }
+                                else if (!flat)
+                                {
+                                        type = 2;
+                                        for (int i = 0; i < N; ++i)
+                                        {
+                                                if (dots[i] < 0)
+                                                {
+                                                        type |= 1 << (2 + i);
+                                                }
+                                        }
+                                }
+                                m.ntype[f] = type;
+                        }
                 }
         });
         if (bad.load() >= 0)
@@ -839,6 +906,9 @@ MeshDev<N> mesh_dev(const MeshHost& m)
         d.rec64 = m.d_rec64.as<double>();
         d.nodes = m.d_nodes.as<int2>();
         d.leaf_idx = m.d_idx.as<int>();
+        d.vnormals = m.ntype.empty() ? nullptr : m.d_normals.as<float>();
+        d.fnormals = m.ntype.empty() ? nullptr : m.d_fnormals.as<int>();
+        d.ntype = m.ntype.empty() ? nullptr : m.d_ntype.as<int>();
         d.nfacets = (int)(m.facets.size() / N);
         d.levels = (int)(m.level_sizes.size() / N);
         for (int k = 0; k < N; ++k)
@@ -912,6 +982,12 @@ void build_scene(nt_scene* s, unsigned threads, bool host_only)
                         m.d_rec64.upload(m.rec64, s->stream);
                         m.d_nodes.upload(m.nodes, s->stream);
                         m.d_idx.upload(m.leaf_idx, s->stream);
+                        if (!m.ntype.empty())
+                        {
+                                m.d_normals.upload(m.normals, s->stream);
+                                m.d_fnormals.upload(m.facet_normals, s->stream);
+                                m.d_ntype.upload(m.ntype, s->stream);
+                        }
                         check_cuda(cudaStreamSynchronize(s->stream), "upload");
                         if (m.pinned)
                         {
@@ -1170,6 +1246,24 @@ int one_dimension_size(int n, int spp)
         return (int)std::ceil(v);
 }
 
+// smooth_normal matters only for meshes with vertex normals (without them the shading normal is the
+// geometric one, as in the reference); then the wavefront carries the smooth-normal shadow queue
+bool smooth_shading(const nt_scene* s, const nt_render_opts& o)
+{
+        if (!o.smooth_normal)
+        {
+                return false;
+        }
+        for (const MeshHost& m : s->meshes)
+        {
+                if (!m.ntype.empty())
+                {
+                        return true;
+                }
+        }
+        return false;
+}
+
 // One pass of samples_per_pixel; moments_accum: per-path sums (pixel * spp_eff + sample, 3 doubles
 // each, zeroed by the caller) instead of the scene's per-pixel accumulator (nt_render_moments).
 template <int N>
@@ -1194,7 +1288,8 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
         std::memcpy(&S, s->dev_scene.data(), sizeof(S));
         S.max_depth = o.max_depth;
         S.retest = o.retest;
-        S.smooth_normal = o.smooth_normal;
+        const bool smooth = smooth_shading(s, o);
+        S.smooth_normal = smooth ? 1 : 0;
         const long long npix = s->pixel_count();
         const long long total = npix * spp_eff;
         if ((s->samples_done + spp_eff) * npix >= (1ll << 62) || s->samples_done + spp_eff > 0xffffffffll)
@@ -1203,17 +1298,19 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
         }
         const int lights = (int)s->lights.size();
         // default pool: 4 Mi paths (fewer wavefront iterations, so less per-launch tail), at most 1 GiB
-        const long long per_path = (long long)(Wavefront<N>::bytes_for(1, lights) - Wavefront<N>::bytes_for(0, lights));
+        const long long per_path =
+                (long long)(Wavefront<N>::bytes_for(1, lights, smooth) - Wavefront<N>::bytes_for(0, lights, smooth));
         long long Q = o.pool_paths > 0 ? o.pool_paths : std::min<long long>(1ll << 22, (1ll << 30) / per_path);
         Q = std::max<long long>(256, std::min(Q, total));
-        if (Q > s->pool_paths || lights > s->pool_lights)
+        if (Q > s->pool_paths || lights > s->pool_lights || (smooth && !s->pool_smooth))
         {
-                s->pool.alloc(Wavefront<N>::bytes_for(Q, lights));
+                s->pool.alloc(Wavefront<N>::bytes_for(Q, lights, smooth));
                 s->pool_paths = Q;
                 s->pool_lights = lights;
+                s->pool_smooth = smooth;
         }
         Wavefront<N> W;
-        W.carve(s->pool.as<char>(), s->pool_paths, s->pool_lights);
+        W.carve(s->pool.as<char>(), s->pool_paths, s->pool_lights, smooth);
 
         PassDev P{};
         P.key0 = (uint32_t)o.seed;
@@ -1312,8 +1409,9 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
                 fail(NT_EINVAL, "sample count overflow");
         }
         const int lights = (int)s->lights.size();
-        const size_t fixed = Wavefront<N>::bytes_for(0, lights);
-        const size_t per_path = Wavefront<N>::bytes_for(1, lights) - fixed;
+        const bool smooth = smooth_shading(s, o);
+        const size_t fixed = Wavefront<N>::bytes_for(0, lights, smooth);
+        const size_t per_path = Wavefront<N>::bytes_for(1, lights, smooth) - fixed;
         const size_t head = 256;  // device counters
         const long long capacity =
                 scratch_bytes > head + fixed ? (long long)((scratch_bytes - head - fixed) / per_path) : 0;
@@ -1334,10 +1432,10 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
         std::memcpy(&S, s->dev_scene.data(), sizeof(S));
         S.max_depth = o.max_depth;
         S.retest = o.retest;
-        S.smooth_normal = o.smooth_normal;
+        S.smooth_normal = smooth ? 1 : 0;
         unsigned long long* counters = static_cast<unsigned long long*>(scratch);
         Wavefront<N> W;
-        W.carve(static_cast<char*>(scratch) + head, Q, lights);
+        W.carve(static_cast<char*>(scratch) + head, Q, lights, smooth);
         PassDev P{};
         P.key0 = (uint32_t)o.seed;
         P.key1 = (uint32_t)(o.seed >> 32);
@@ -1633,6 +1731,38 @@ int nt_scene_add_mesh(nt_scene* scene, const float* vertices, int64_t vertex_cou
                 m.surface = surface_or_default(surface);
                 scene->meshes.push_back(std::move(m));
                 scene->objects.push_back({OBJ_MESH, (int)scene->meshes.size() - 1});
+                scene->built = false;
+        });
+}
+
+int nt_scene_set_mesh_normals(nt_scene* scene, int object, const float* normals, int64_t normal_count,
+                              const int32_t* facet_normals)
+{
+        return guarded([&]() {
+                need_scene(scene);
+                if (object < 0 || object >= (int)scene->objects.size() || scene->objects[object].kind != OBJ_MESH)
+                {
+                        fail(NT_EINVAL, "object is not a mesh");
+                }
+                if (!normals || normal_count < 1)
+                {
+                        fail(NT_EINVAL, "no normals");
+                }
+                const int n = scene->n;
+                MeshHost& m = scene->meshes[scene->objects[object].index];
+                std::vector<float> nv = vec_copy(normals, (size_t)normal_count * n, "normals");
+                std::vector<int32_t> fn = facet_normals ? std::vector<int32_t>(facet_normals, facet_normals + m.facets.size())
+                                                        : m.facets;
+                for (int32_t i : fn)
+                {
+                        if (i < 0 || i >= normal_count)
+                        {
+                                fail(NT_EINVAL, "facet normal index out of range");
+                        }
+                }
+                m.normals = std::move(nv);
+                m.facet_normals = std::move(fn);
+                m.ready = false;
                 scene->built = false;
         });
 }

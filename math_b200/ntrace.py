@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = (
     "nt_scene_set_projector", "nt_scene_set_background", "nt_scene_build", "nt_scene_mesh_info", "nt_render",
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
-    "nt_scene_upload", "nt_scene_stream", "nt_scene_clear_lights", "nt_scene_set_object_surface", "nt_render_aux",
+    "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_clear_lights", "nt_scene_set_object_surface", "nt_render_aux",
     "nt_render_moments", "nt_render_noalloc",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
     "nt_denoiser_set_params", "nt_denoiser_set_input", "nt_denoiser_apply", "nt_denoiser_gradient",
@@ -130,6 +130,7 @@ def library() -> ctypes.CDLL:
         "nt_last_error_message": ([], ctypes.c_char_p),
         "nt_effective_spp": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "nt_cosine_sphere_coefficient": ([ctypes.c_int], ctypes.c_double),
+        "nt_scene_set_mesh_normals": ([vp, ctypes.c_int, f32p, i64, i32p], ctypes.c_int),
         "nt_scene_clear_lights": ([vp], ctypes.c_int),
         "nt_scene_set_object_surface": ([vp, ctypes.c_int, ctypes.POINTER(Surface)], ctypes.c_int),
         "nt_render_aux": ([vp, vp, vp, vp], ctypes.c_int),
@@ -304,6 +305,14 @@ class Scene:
         spp = ctypes.c_int64()
         _check(self._lib.nt_accum_read(self._h, out.ctypes.data, ctypes.byref(spp)))
         return out, int(spp.value)
+
+    def set_mesh_normals(self, obj: int, normals, facet_normals=None) -> None:
+        """Vertex normals of mesh object `obj` (normal_count x n) and optional per-facet normal indices
+        (facet_count x n; default: the facets' vertex indices); used with smooth_normal."""
+        nv = _f32(normals).reshape(-1, self.n)
+        fn = None if facet_normals is None else np.ascontiguousarray(np.asarray(facet_normals, np.int32))
+        _check(self._lib.nt_scene_set_mesh_normals(self._h, int(obj), nv.ctypes.data, len(nv),
+                                                   None if fn is None else fn.ctypes.data))
 
     def clear_lights(self) -> None:
         """Removes every light (add new ones, then build again; the meshes' trees are kept)."""

@@ -157,6 +157,8 @@ def build_scene(spec: dict, threads: int = 0) -> ntrace.Scene:
     s = ntrace.Scene(n)
     if spec["verts"] is not None:
         s.add_mesh(spec["verts"], spec["facets"], color=spec["mesh_color"], diffuse=spec["mesh_diffuse"])
+        if spec.get("normals") is not None:
+            s.set_mesh_normals(0, spec["normals"], spec.get("facet_normals"))
     if spec["floor"] is not None:
         fl = spec["floor"]
         s.add_parallelotope(fl["org"], fl["edges"], color=fl["color"], diffuse=fl["diffuse"])

@@ -45,6 +45,7 @@ class SceneStruct(ctypes.Structure):
         ("screen_axes", ctypes.c_float * 30), ("proj_param", ctypes.c_float), ("screen", ctypes.c_int * 5),
         ("bg_color", ctypes.c_float * 3), ("bg_light_color", ctypes.c_float * 3), ("bg_is_light", ctypes.c_int),
         ("smooth_normal", ctypes.c_int), ("tree_threads", ctypes.c_int),
+        ("normals", ctypes.c_void_p), ("nnormals", ctypes.c_long), ("facet_normals", ctypes.c_void_p),
     ]
 
 
@@ -114,8 +115,16 @@ def scene_struct(spec: dict, dbl: bool, threads: int = 1) -> tuple[SceneStruct, 
         s.bg_color[i] = bg["color"][i]
         s.bg_light_color[i] = bg["light_color"][i]
     s.bg_is_light = int(bg["light"])
-    s.smooth_normal = 0
+    s.smooth_normal = int(bool(spec.get("smooth_normal", False)))
     s.tree_threads = threads
+    if spec.get("normals") is not None:
+        nv = np.ascontiguousarray(spec["normals"], dtype=np.float32).reshape(-1, n)
+        keep.append(nv)
+        s.normals, s.nnormals = nv.ctypes.data, len(nv)
+        if spec.get("facet_normals") is not None:
+            fn = np.ascontiguousarray(spec["facet_normals"], dtype=np.int32).reshape(-1, n)
+            keep.append(fn)
+            s.facet_normals = fn.ctypes.data
     return s, keep
 
 

@@ -455,6 +455,8 @@ static double now_seconds(void)
                         stats->shadow_rays = job.total.shadow_rays;                                               \
                         stats->seconds = t1 - t0;                                                                 \
                 }                                                                                                 \
+                free(scene.ntype);                                                                                \
+                free(scene.nsign);                                                                                \
                 mesh_free_##S(mesh);                                                                              \
                 return 0;                                                                                         \
         }

@@ -60,6 +60,10 @@ typedef struct ort_scene
         int bg_is_light;
         int smooth_normal;
         int tree_threads;
+        /* optional vertex normals of the mesh (nnormals == 0: none); facet_normals NULL: vertex indices */
+        const float* normals;
+        long nnormals;
+        const int* facet_normals;
 } ort_scene;
 
 typedef struct ort_stats

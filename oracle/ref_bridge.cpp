@@ -183,9 +183,111 @@ struct MeshHandle final : MeshHandleBase
         std::shared_ptr<const Mesh<N, T>> mesh;
 };
 
-template <size_t N, typename T>
-MeshHandleBase* mesh_create(const float* verts, long nverts, const int* facets, long nfacets, int threads)
+// An Obj<N> (src/obj/obj.h) holding the caller's vertices, vertex normals and facets as given (the
+// reference's create_obj_for_facets with normals averages them with the face normals; the mesh with
+// vertex normals here must take them unchanged, as the product's nt_scene_set_mesh_normals does).
+template <size_t N>
+class NormalsObj final : public Obj<N>
 {
+        std::vector<Vector<N, float>> m_vertices;
+        std::vector<Vector<N, float>> m_normals;
+        std::vector<Vector<N - 1, float>> m_texcoords;
+        std::vector<typename Obj<N>::Facet> m_facets;
+        std::vector<typename Obj<N>::Point> m_points;
+        std::vector<typename Obj<N>::Line> m_lines;
+        std::vector<typename Obj<N>::Material> m_materials;
+        std::vector<typename Obj<N>::Image> m_images;
+
+public:
+        NormalsObj(const float* verts, long nverts, const int* facets, long nfacets, const float* normals, long nnormals,
+                   const int* facet_normals)
+                : m_vertices(nverts), m_normals(nnormals), m_facets(nfacets)
+        {
+                for (long i = 0; i < nverts; ++i)
+                {
+                        for (unsigned k = 0; k < N; ++k)
+                        {
+                                m_vertices[i][k] = verts[i * N + k];
+                        }
+                }
+                for (long i = 0; i < nnormals; ++i)
+                {
+                        for (unsigned k = 0; k < N; ++k)
+                        {
+                                m_normals[i][k] = normals[i * N + k];
+                        }
+                }
+                for (long f = 0; f < nfacets; ++f)
+                {
+                        typename Obj<N>::Facet& fc = m_facets[f];
+                        fc.material = -1;
+                        fc.has_texcoord = false;
+                        fc.has_normal = true;
+                        for (unsigned i = 0; i < N; ++i)
+                        {
+                                fc.vertices[i] = facets[f * N + i];
+                                fc.normals[i] = facet_normals ? facet_normals[f * N + i] : facets[f * N + i];
+                                fc.texcoords[i] = -1;
+                        }
+                }
+        }
+        const std::vector<Vector<N, float>>& vertices() const override
+        {
+                return m_vertices;
+        }
+        const std::vector<Vector<N, float>>& normals() const override
+        {
+                return m_normals;
+        }
+        const std::vector<Vector<N - 1, float>>& texcoords() const override
+        {
+                return m_texcoords;
+        }
+        const std::vector<typename Obj<N>::Facet>& facets() const override
+        {
+                return m_facets;
+        }
+        const std::vector<typename Obj<N>::Point>& points() const override
+        {
+                return m_points;
+        }
+        const std::vector<typename Obj<N>::Line>& lines() const override
+        {
+                return m_lines;
+        }
+        const std::vector<typename Obj<N>::Material>& materials() const override
+        {
+                return m_materials;
+        }
+        const std::vector<typename Obj<N>::Image>& images() const override
+        {
+                return m_images;
+        }
+        Vector<N, float> center() const override
+        {
+                return Vector<N, float>(0);
+        }
+        float length() const override
+        {
+                return 1;
+        }
+};
+
+template <size_t N, typename T>
+MeshHandleBase* mesh_create(const float* verts, long nverts, const int* facets, long nfacets, int threads,
+                            const float* normals = nullptr, long nnormals = 0, const int* facet_normals = nullptr)
+{
+        if (normals && nnormals > 0)
+        {
+                NormalsObj<N> obj(verts, nverts, facets, nfacets, normals, nnormals, facet_normals);
+                ProgressRatio progress(nullptr);
+                constexpr Matrix<N + 1, N + 1, T> matrix(1);
+                auto h = std::make_unique<MeshHandle<N, T>>();
+                h->n = N;
+                h->dbl = std::is_same_v<T, double>;
+                h->mesh = std::make_shared<const Mesh<N, T>>(&obj, matrix, threads, &progress);
+                return h.release();
+        }
         std::vector<Vector<N, float>> points(nverts);
         for (long i = 0; i < nverts; ++i)
         {
@@ -330,6 +432,10 @@ struct refb_scene
         int bg_is_light;
         int smooth_normal;
         int tree_threads;
+        // optional vertex normals of the mesh (nnormals == 0: none); facet_normals NULL: vertex indices
+        const float* normals;
+        long nnormals;
+        const int* facet_normals;
 };
 
 struct refb_stats
@@ -573,8 +679,9 @@ int paint_impl(const refb_scene& s, int spp, int max_depth, unsigned long long s
         std::shared_ptr<const Mesh<N, T>> mesh;
         if (s.nfacets > 0)
         {
-                std::unique_ptr<MeshHandleBase> h(
-                        mesh_create<N, T>(s.verts, s.nverts, s.facets, s.nfacets, std::max(1, s.tree_threads)));
+                std::unique_ptr<MeshHandleBase> h(mesh_create<N, T>(s.verts, s.nverts, s.facets, s.nfacets,
+                                                                    std::max(1, s.tree_threads), s.normals, s.nnormals,
+                                                                    s.facet_normals));
                 mesh = static_cast<MeshHandle<N, T>*>(h.get())->mesh;
         }
         BridgeScene<N, T> scene(s, mesh);

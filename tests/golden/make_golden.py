@@ -15,6 +15,8 @@ Fixtures (numpy .npz, small enough to commit):
                             per pixel, painted twice with different seeds (one thread, seeded engines),
                             so that a test can compare another renderer's image against the reference
                             with the reference's own run-to-run noise as the yardstick.
+  radiance_n3_smooth.npz   - the same, the view closed in on the sphere (2.4 x 2.4), with vertex
+                            normals of every NormalType and smooth_normal set (smooth_mesh below).
 """
 
 from __future__ import annotations
@@ -103,8 +105,45 @@ def radiance_fixture(ref: checkers.Reference) -> None:
     print(f"radiance: {img_a.shape}, run-to-run relative RMSE {rr:.4g}, {time.time() - t0:.1f}s")
 
 
+def smooth_mesh(subdivisions: int = 2, seed: int = 5) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """An icosphere with vertex normals that exercise every NormalType of MeshHyperplaneSimplex
+    (mesh_hyperplane_simplex.cpp:96-143): sphere normals (Use), every 5th facet wound backwards (all
+    vertex normals opposite the facet normal: Use with the facet normal reversed), every 11th vertex
+    normal negated (mixed signs: Reverse), every 13th vertex normal tilted by 60 degrees (|cos| < 0.7:
+    None)."""
+    rng = np.random.default_rng(seed)
+    verts, facets = scenes.icosphere(subdivisions)
+    normals = verts / np.linalg.norm(verts, axis=1, keepdims=True)
+    facets = facets.copy()
+    facets[::5, [0, 1]] = facets[::5, [1, 0]]
+    normals[::11] *= -1
+    for i in range(0, len(normals), 13):
+        t = rng.standard_normal(3)
+        t -= np.dot(t, normals[i]) * normals[i]
+        t /= np.linalg.norm(t)
+        normals[i] = 0.5 * normals[i] + np.sqrt(0.75) * t
+    return verts.astype(np.float32), facets.astype(np.int32), normals.astype(np.float32)
+
+
+def radiance_smooth_fixture(ref: checkers.Reference) -> None:
+    verts, facets, normals = smooth_mesh()
+    spec = scenes.make_spec(3, verts, facets, screen=24, spp=1024, max_depth=5, extent=2.4)
+    spec["normals"] = normals
+    spec["smooth_normal"] = True
+    t0 = time.time()
+    img_a, st_a = ref.paint(spec, dbl=True, seed=1, threads=8)
+    img_b, st_b = ref.paint(spec, dbl=True, seed=2, threads=8)
+    np.savez_compressed(OUT / "radiance_n3_smooth.npz", verts=verts, facets=facets, normals=normals, screen=24,
+                        extent=2.4, spp=1024, max_depth=5, image_a=img_a, image_b=img_b,
+                        samples=st_a["sample_count"])
+    rr = np.sqrt(((img_a - img_b) ** 2).sum() / (img_b ** 2).sum())
+    print(f"radiance (smooth normals): {img_a.shape}, run-to-run relative RMSE {rr:.4g}, {time.time() - t0:.1f}s")
+
+
 if __name__ == "__main__":
     checkers.build()
     reference = checkers.Reference()
-    closest_fixtures(reference)
-    radiance_fixture(reference)
+    if "--smooth-only" not in sys.argv:
+        closest_fixtures(reference)
+        radiance_fixture(reference)
+    radiance_smooth_fixture(reference)

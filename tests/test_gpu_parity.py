@@ -159,6 +159,48 @@ def test_radiance_matches_reference_statistically(require_gpu):
     assert rrmse(img, b) < 1.5 * noise
 
 
+def _smooth_spec():
+    from math_b200 import scenes
+
+    g = np.load(GOLDEN / "radiance_n3_smooth.npz")
+    spec = scenes.make_spec(3, g["verts"], g["facets"], screen=int(g["screen"]), spp=int(g["spp"]),
+                            max_depth=int(g["max_depth"]), extent=float(g["extent"]))
+    spec["normals"] = g["normals"]
+    spec["smooth_normal"] = True
+    return spec, g
+
+
+def test_smooth_normal_radiance_matches_oracle_paths(require_gpu, port):
+    """Vertex normals of every NormalType with smooth_normal: the same Philox paths as the oracle's
+    float painter (interpolated shading normals, the smooth-normal shadow branch)."""
+    from math_b200 import scenes
+
+    spec, _ = _smooth_spec()
+    s = scenes.build_scene(spec)
+    st = s.render(64, max_depth=5, seed=3, smooth_normal=True)
+    img, _ = s.image()
+    assert st["error_bits"] == 0
+    p32, _ = port.paint(spec, dbl=False, spp=64, seed=3, threads=8)
+    assert rrmse(img, p32) < 1e-4
+    s.clear()
+    s.render(64, max_depth=5, seed=3, smooth_normal=False)
+    flat, _ = s.image()
+    assert rrmse(flat, img) > 1e-2
+
+
+def test_smooth_normal_radiance_matches_reference_statistically(require_gpu):
+    from math_b200 import scenes
+
+    spec, g = _smooth_spec()
+    s = scenes.build_scene(spec)
+    s.render(int(g["spp"]), max_depth=int(g["max_depth"]), seed=777, smooth_normal=True)
+    img, _ = s.image()
+    a, b = g["image_a"], g["image_b"]
+    noise = rrmse(a, b)
+    assert rrmse(img, a) < 1.5 * noise
+    assert rrmse(img, b) < 1.5 * noise
+
+
 def test_progressive_passes_accumulate(require_gpu):
     """Two passes of k samples continue the sample sequence: equal to the oracle painting 2k with an
     offset, and the sample count adds up."""

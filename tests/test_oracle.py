@@ -164,3 +164,24 @@ def test_port_radiance_matches_reference_statistically(port):
     noise = np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum())
     diff = np.sqrt(((img - a) ** 2).sum() / (a ** 2).sum())
     assert diff < 1.5 * noise
+
+
+def test_port_smooth_normal_radiance_matches_reference_statistically(port):
+    """Vertex normals of every NormalType with smooth_normal set (shading-normal interpolation and the
+    smooth-normal shadow branch, painter.cpp:238-284): the oracle against the reference's paint()."""
+    from math_b200 import scenes
+
+    g = np.load(GOLDEN / "radiance_n3_smooth.npz")
+    spec = scenes.make_spec(3, g["verts"], g["facets"], screen=int(g["screen"]), spp=int(g["spp"]),
+                            max_depth=int(g["max_depth"]), extent=float(g["extent"]))
+    spec["normals"] = g["normals"]
+    spec["smooth_normal"] = True
+    img, _ = port.paint(spec, dbl=True, threads=4)
+    a, b = g["image_a"], g["image_b"]
+    noise = np.sqrt(((a - b) ** 2).sum() / (b ** 2).sum())
+    diff = np.sqrt(((img - a) ** 2).sum() / (a ** 2).sum())
+    assert diff < 1.5 * noise, (diff, noise)
+    # the flat-shaded image is far outside that noise: the test sees the smooth shading
+    flat = dict(spec, smooth_normal=False)
+    img_flat, _ = port.paint(flat, dbl=True, threads=4)
+    assert np.sqrt(((img_flat - a) ** 2).sum() / (a ** 2).sum()) > 5 * noise
