@@ -67,8 +67,10 @@ typedef struct nt_render_opts
         int retest;             /* 1: re-test uncertain FP32 facet tests in FP64 (default); 0: FP32 only */
         int smooth_normal;      /* paint()'s smooth_normal; meshes without vertex normals ignore it */
         int64_t pool_paths;     /* wavefront path pool size; <= 0: automatic */
-        int timing;             /* 1: per-kernel CUDA-event times in nt_stats */
-        const volatile int* stop; /* optional host stop flag, polled between wavefront iterations */
+        int timing;             /* 1: per-kernel CUDA-event times in nt_stats (iterations enqueued one by one) */
+        const volatile int* stop; /* optional host stop flag, polled between batches of wavefront iterations */
+        int graph_iterations;   /* wavefront iterations per CUDA-graph launch (the host checks for the end of
+                                   the pass after each); <= 0: 4.  nt_autotune picks it with pool_paths. */
 } nt_render_opts;
 
 typedef struct nt_stats
@@ -95,6 +97,7 @@ typedef struct nt_stats
         int64_t shadow_box_steps;
         int64_t shadow_retests;
         int64_t shadow_descent_levels;
+        int64_t iterations;       /* wavefront iterations that had work */
 } nt_stats;
 
 typedef struct nt_mesh_info
@@ -197,6 +200,20 @@ int nt_render_noalloc(nt_scene* scene, const nt_render_opts* opts, double* d_acc
                       void* stream, nt_stats* stats);
 
 int nt_accum_clear(nt_scene* scene);
+
+/* ---- batches and tuning (no counterpart in the reference, which paints one scene per call) ---- */
+
+/* One pass of each of `count` built scenes (distinct; any mix of dimensions), opts[i] for scene i,
+ * run side by side: the wavefront iterations of all the passes, each on its scene's stream, are
+ * captured into one CUDA graph, and the graph is launched until every pass has finished (a pass
+ * that ends first idles through empty iterations).  stats: count entries, or NULL. */
+int nt_render_batch(nt_scene* const* scenes, int count, const nt_render_opts* opts, nt_stats* stats);
+
+/* Times probe passes of `base` (its samples per pixel) over candidate path-pool sizes and iterations
+ * per graph launch and returns the fastest in *tuned (a copy of base with pool_paths and
+ * graph_iterations set) and its pass time in *best_ms (may be NULL).  The probe passes go to the
+ * scene's accumulator, which is cleared afterwards. */
+int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tuned, double* best_ms);
 
 /* ---- denoiser inputs (no counterpart in the reference; see include/ntrace_denoise.h) ---- */
 

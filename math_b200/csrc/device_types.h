@@ -176,8 +176,15 @@ enum Counter : int
         // work cursors of the persistent extension and shadow kernels
         C_WORK_EXT = 13,
         C_WORK_SH = 14,
-        C_SMOOTH = 15,  // entries of the smooth-normal shadow queue
-        C_COUNT = 16
+        C_SMOOTH = 15,     // entries of the smooth-normal shadow queue
+        // wavefront control, kept on the device so that iterations need no host round trip
+        C_Q_ACTIVE = 16,   // paths in the current queue
+        C_Q_NEXT = 17,     // next fresh path of the pass (relative to PassDev::path_begin)
+        C_Q_FRESH = 18,    // fresh paths generated by this iteration
+        C_Q_BASE = 19,     // queue slot of the first fresh path
+        C_DONE = 20,       // 1 once every path of the pass has finished
+        C_ITERS = 21,      // iterations that had work
+        C_COUNT = 24
 };
 
 enum ErrorBits : int

@@ -198,15 +198,9 @@ struct ShadowView
 // paint_pixels: stratified jittered sample -> projector ray (painter.cpp:410-448,
 // sampler.h:26-64, engine.h:86-156)
 template <int N>
-__global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, long long first_slot,
-                                                  long long count)
+__device__ __forceinline__ void raygen_one(const DevScene<N>& S, const PassDev& P, const PathView<N>& A, long long g,
+                                           long long slot)
 {
-        long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (i >= count)
-        {
-                return;
-        }
-        long long g = P.path_begin + i;
         long long pixel = g / P.spp_eff;
         int s = (int)(g - pixel * P.spp_eff);
         long long sample = P.sample_offset + s;
@@ -244,7 +238,6 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevSce
         }
         Ray<N> ray;
         projector_ray<N>(S.proj, point, ray);
-        long long slot = first_slot + i;
 #pragma unroll
         for (int k = 0; k < N; ++k)
         {
@@ -258,6 +251,20 @@ __global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevSce
         A.pix[slot] = P.moments ? (uint32_t)g : (uint32_t)pixel;
         A.smp[slot] = (uint32_t)sample;
         A.level[slot] = 0;
+}
+
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_raygen(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A,
+                                                  const unsigned long long* __restrict__ ctl)
+{
+        // this iteration's fresh paths (k_iter_begin): queue slots base.., pass paths first..
+        const long long fresh = (long long)ctl[C_Q_FRESH];
+        const long long base = (long long)ctl[C_Q_BASE];
+        const long long first = (long long)ctl[C_Q_NEXT] - fresh;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < fresh; i += (long long)gridDim.x * blockDim.x)
+        {
+                raygen_one<N>(S, P, A, P.path_begin + first + i, base + i);
+        }
 }
 
 // Persistent warps take 32 consecutive rays at a time from a device counter until the queue is
@@ -274,9 +281,10 @@ __device__ __forceinline__ long long warp_take(unsigned long long* work)
 
 // extension: closest object per path (ray_intersection over objects, ray_intersection.h:26-105)
 template <int N>
-__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, long long count,
+__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H,
                                                   unsigned long long* counters)
 {
+        const long long count = (long long)counters[C_Q_ACTIVE];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
         for (long long base = warp_take(counters + C_WORK_EXT); base < count; base = warp_take(counters + C_WORK_EXT))
@@ -323,8 +331,9 @@ __device__ __forceinline__ void accumulate(double* accum, uint32_t pixel, float 
 template <int N>
 __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, HitView<N> H,
                                                  PathView<N> B, ShadowView<N> SQ, ShadowView<N> SM, double* accum,
-                                                 long long count, unsigned long long* counters)
+                                                 unsigned long long* counters)
 {
+        const long long count = (long long)counters[C_Q_ACTIVE];
         __shared__ int s_warp[BLOCK / 32];
         __shared__ long long s_base;
         const long long tiles = (count + blockDim.x - 1) / blockDim.x;
@@ -576,9 +585,10 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
 
 // shadow rays: light_source_is_visible (painter.cpp:172-186); visible -> add the light's share
 template <int N>
-__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, long long count,
+__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum,
                                                   unsigned long long* counters)
 {
+        const long long count = (long long)counters[C_SHADOW];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
         for (long long base = warp_take(counters + C_WORK_SH); base < count; base = warp_take(counters + C_WORK_SH))
@@ -611,12 +621,12 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_consta
 // normals, only with smooth_normal), so one ray per thread through the general scene functions.
 template <int N>
 __global__ void __launch_bounds__(BLOCK) k_shadow_smooth(__grid_constant__ const DevScene<N> S, ShadowView<N> SM,
-                                                         double* accum, long long count, unsigned long long* counters)
+                                                         double* accum, unsigned long long* counters)
 {
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
-        const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-        if (i < count)
+        const long long count = (long long)counters[C_SMOOTH];
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
         {
                 Ray<N> r;
 #pragma unroll
@@ -628,7 +638,7 @@ __global__ void __launch_bounds__(BLOCK) k_shadow_smooth(__grid_constant__ const
                 const float dist = SM.at(2 * N, i);
                 float t, t_rev;
                 int obj, facet;
-                rays = 1;
+                rays += 1;
                 bool lit = false;
                 if (scene_closest<N>(S, r, &t, &obj, &facet, &ws) && t < dist)
                 {
@@ -640,11 +650,11 @@ __global__ void __launch_bounds__(BLOCK) k_shadow_smooth(__grid_constant__ const
                                 rev.dir[k] = -r.dir[k];
                         }
                         ray_move<N>(rev, 2 * S.ray_offset);
-                        rays = 2;
+                        rays += 1;
                         if (!(scene_closest<N>(S, rev, &t_rev, &obj, &facet, &ws) && t_rev < t))
                         {
                                 ray_move<N>(r, t + S.ray_offset);
-                                rays = 3;
+                                rays += 1;
                                 lit = scene_visible<N>(S, r, dist - t, &ws);
                         }
                 }
@@ -691,9 +701,9 @@ __device__ __forceinline__ long long lane_refill(bool idle, unsigned long long* 
 // Extension rays of a scene with one mesh: closest_plan at fetch, then one leaf per iteration.
 template <int N>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
-        k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, long long count,
-                        unsigned long long* counters)
+        k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, unsigned long long* counters)
 {
+        const long long count = (long long)counters[C_Q_ACTIVE];
         const MeshDev<N>& M = S.mesh[0];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
@@ -779,9 +789,9 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
 // otherwise the mesh is walked (up to the light's distance) when its root box starts before the light.
 template <int N>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
-        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, long long count,
-                        unsigned long long* counters)
+        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, unsigned long long* counters)
 {
+        const long long count = (long long)counters[C_SHADOW];
         const MeshDev<N>& M = S.mesh[0];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
@@ -986,6 +996,38 @@ __global__ void k_moments_reduce(long long npix, int spp, const double* __restri
         }
 }
 
+// Start of a wavefront iteration (one thread): refill the queue with fresh paths up to Q and clear the
+// per-iteration counters.
+__global__ void k_iter_begin(unsigned long long* c, long long total, long long Q)
+{
+        const long long active = (long long)c[C_Q_ACTIVE];
+        const long long next = (long long)c[C_Q_NEXT];
+        long long fresh = Q - active < total - next ? Q - active : total - next;
+        fresh = fresh > 0 ? fresh : 0;
+        c[C_Q_BASE] = (unsigned long long)active;
+        c[C_Q_FRESH] = (unsigned long long)fresh;
+        c[C_Q_ACTIVE] = (unsigned long long)(active + fresh);
+        c[C_Q_NEXT] = (unsigned long long)(next + fresh);
+        c[C_WORK_EXT] = 0;
+        c[C_WORK_SH] = 0;
+        c[C_ACTIVE_OUT] = 0;
+        c[C_SHADOW] = 0;
+        c[C_SMOOTH] = 0;
+        if (active + fresh > 0)
+        {
+                c[C_ITERS] += 1;
+        }
+}
+
+// End of an iteration (one thread): the continuations become the queue; done once every path of the
+// pass has been generated and finished.
+__global__ void k_iter_end(unsigned long long* c, long long total)
+{
+        const long long survivors = (long long)c[C_ACTIVE_OUT];
+        c[C_Q_ACTIVE] = (unsigned long long)survivors;
+        c[C_DONE] = (survivors == 0 && (long long)c[C_Q_NEXT] >= total) ? 1ull : 0ull;
+}
+
 template <int N>
 long long grid_for(long long count)
 {
@@ -1054,139 +1096,208 @@ void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
 }
 
 template <int N>
-cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
-                              unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
-                              bool timing, const volatile int* stop)
+void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, double* accum, unsigned long long* counters,
+                                     long long total_paths, int parity, cudaStream_t st, KernelTimes* times,
+                                     cudaEvent_t* ev) const
 {
-        long long active = 0;
-        long long next = 0;
-        bool flip = false;
-        cudaEvent_t ev[8];
-        if (timing)
-        {
-                for (auto& e : ev)
-                {
-                        cudaEventCreate(&e);
-                }
-        }
-        const long long path_base = P.path_begin;
         static const long long extend_blocks = resident_blocks(k_extend<N>);
         static const long long shadow_blocks = resident_blocks(k_shadow<N>);
         static const long long extend_refill_blocks = resident_blocks(k_extend_refill<N>);
         static const long long shadow_refill_blocks = resident_blocks(k_shadow_refill<N>);
+        static const long long stream_blocks = resident_blocks(k_shade<N>);
         // scenes with exactly one mesh use the lane-refill walk kernels
         const bool one_mesh = S.nmesh == 1;
-        for (int iter = 0; active > 0 || next < total_paths; ++iter)
+        const bool smooth = S.smooth_normal != 0;
+        const long long walk_cap = std::max<long long>(1, (Q * lights + BLOCK - 1) / BLOCK);
+        const unsigned ext_grid = (unsigned)std::min(one_mesh ? extend_refill_blocks : extend_blocks, walk_cap);
+        const unsigned sh_grid = (unsigned)std::min(one_mesh ? shadow_refill_blocks : shadow_blocks, walk_cap);
+        const unsigned str_grid = (unsigned)std::min(stream_blocks * 2, walk_cap);
+        const bool flip = parity != 0;
+        float* fa = flip ? fB : fA;
+        float* fb = flip ? fA : fB;
+        PathView<N> A{fa, flip ? pixB : pixA, flip ? smpB : smpA, flip ? lvlB : lvlA, Q};
+        PathView<N> B{fb, flip ? pixA : pixB, flip ? smpA : smpB, flip ? lvlA : lvlB, Q};
+        HitView<N> H{hit_t, hit_obj, hit_facet};
+        ShadowView<N> SQ{sq_f, sq_pix, Q * lights};
+        ShadowView<N> SM{sm_f, sm_pix, Q * lights};
+        k_iter_begin<<<1, 1, 0, st>>>(counters, total_paths, Q);
+        if (ev)
+        {
+                cudaEventRecord(ev[0], st);
+        }
+        k_raygen<N><<<str_grid, BLOCK, 0, st>>>(S, P, A, counters);
+        if (ev)
+        {
+                cudaEventRecord(ev[1], st);
+        }
+        if (one_mesh)
+        {
+                k_extend_refill<N><<<ext_grid, BLOCK, 0, st>>>(S, A, H, counters);
+        }
+        else
+        {
+                k_extend<N><<<ext_grid, BLOCK, 0, st>>>(S, A, H, counters);
+        }
+        if (ev)
+        {
+                cudaEventRecord(ev[2], st);
+        }
+        k_shade<N><<<str_grid, BLOCK, 0, st>>>(S, P, A, H, B, SQ, SM, accum, counters);
+        if (ev)
+        {
+                cudaEventRecord(ev[3], st);
+        }
+        if (one_mesh)
+        {
+                k_shadow_refill<N><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, counters);
+        }
+        else
+        {
+                k_shadow<N><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, counters);
+        }
+        if (smooth)
+        {
+                k_shadow_smooth<N><<<str_grid, BLOCK, 0, st>>>(S, SM, accum, counters);
+        }
+        if (ev)
+        {
+                cudaEventRecord(ev[4], st);
+        }
+        k_iter_end<<<1, 1, 0, st>>>(counters, total_paths);
+        if (times)
+        {
+                times->launches += iteration_launches(smooth);
+                times->extend_launches += 1;
+                times->shadow_launches += 1;
+        }
+}
+
+template <int N>
+cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
+                              unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
+                              bool timing, const volatile int* stop, bool use_graph, int batch)
+{
+        const bool smooth = S.smooth_normal != 0;
+        if (smooth && !sm_f)
+        {
+                return cudaErrorInvalidValue;  // the pool was carved without the smooth-normal queue
+        }
+        // iterations between host checks of the done flag (a pass takes tens of iterations; the few
+        // that run after it is done find empty queues and return at once)
+        const int BATCH = std::max(1, batch);
+        cudaError_t e = cudaMemsetAsync(counters + C_Q_ACTIVE, 0, (C_COUNT - C_Q_ACTIVE) * sizeof(unsigned long long), st);
+        if (e != cudaSuccess)
+        {
+                return e;
+        }
+        cudaGraphExec_t exec = nullptr;
+        if (use_graph && !timing)
+        {
+                // the BATCH iterations are captured once per pass and replayed as one graph launch
+                // (BATCH even, so that the queue parity is the same at the start of every replay)
+                const int even = BATCH + (BATCH & 1);
+                cudaGraph_t graph = nullptr;
+                e = cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal);
+                if (e == cudaSuccess)
+                {
+                        for (int k = 0; k < even; ++k)
+                        {
+                                enqueue_iteration(S, P, accum, counters, total_paths, k & 1, st, nullptr, nullptr);
+                        }
+                        e = cudaStreamEndCapture(st, &graph);
+                        if (e == cudaSuccess)
+                        {
+                                e = cudaGraphInstantiate(&exec, graph, 0);
+                                cudaGraphDestroy(graph);
+                        }
+                }
+                if (e != cudaSuccess)
+                {
+                        // capture unavailable (e.g. the caller's stream is itself being captured):
+                        // enqueue the iterations directly
+                        cudaGetLastError();
+                        exec = nullptr;
+                        e = cudaSuccess;
+                }
+        }
+        cudaEvent_t ev[6];
+        if (timing)
+        {
+                for (auto& v : ev)
+                {
+                        cudaEventCreate(&v);
+                }
+        }
+        const int per_replay = BATCH + (BATCH & 1);
+        int parity = 0;
+        while (true)
         {
                 if (stop && *stop)
                 {
                         break;
                 }
-                float* fa = flip ? fB : fA;
-                float* fb = flip ? fA : fB;
-                PathView<N> A{fa, flip ? pixB : pixA, flip ? smpB : smpA, flip ? lvlB : lvlA, Q};
-                PathView<N> B{fb, flip ? pixA : pixB, flip ? smpA : smpB, flip ? lvlA : lvlB, Q};
-                HitView<N> H{hit_t, hit_obj, hit_facet};
-                ShadowView<N> SQ{sq_f, sq_pix, Q * lights};
-                ShadowView<N> SM{sm_f, sm_pix, Q * lights};
-
-                long long fresh = std::min(Q - active, total_paths - next);
                 if (timing)
                 {
-                        cudaEventRecord(ev[0], st);
+                        for (int k = 0; k < BATCH; ++k)
+                        {
+                                enqueue_iteration(S, P, accum, counters, total_paths, parity, st, times, ev);
+                                parity ^= 1;
+                                cudaEventRecord(ev[5], st);
+                                cudaEventSynchronize(ev[5]);
+                                float ms;
+                                cudaEventElapsedTime(&ms, ev[0], ev[1]);
+                                times->raygen_ms += ms;
+                                cudaEventElapsedTime(&ms, ev[1], ev[2]);
+                                times->extend_ms += ms;
+                                cudaEventElapsedTime(&ms, ev[2], ev[3]);
+                                times->shade_ms += ms;
+                                cudaEventElapsedTime(&ms, ev[3], ev[4]);
+                                times->shadow_ms += ms;
+                        }
                 }
-                if (fresh > 0)
+                else if (exec)
                 {
-                        PassDev pp = P;
-                        pp.path_begin = path_base + next;
-                        k_raygen<N><<<(unsigned)grid_for<N>(fresh), BLOCK, 0, st>>>(S, pp, A, active, fresh);
-                        next += fresh;
-                        active += fresh;
-                }
-                if (timing)
-                {
-                        cudaEventRecord(ev[1], st);
-                }
-                cudaMemsetAsync(counters + C_WORK_EXT, 0, 2 * sizeof(unsigned long long), st);
-                if (one_mesh)
-                {
-                        k_extend_refill<N><<<(unsigned)std::min(extend_refill_blocks, grid_for<N>(active)), BLOCK, 0, st>>>(
-                                S, A, H, active, counters);
+                        e = cudaGraphLaunch(exec, st);
+                        if (e != cudaSuccess)
+                        {
+                                break;
+                        }
+                        times->launches += (long long)per_replay * iteration_launches(smooth);
+                        times->extend_launches += per_replay;
+                        times->shadow_launches += per_replay;
                 }
                 else
                 {
-                        k_extend<N><<<(unsigned)std::min(extend_blocks, grid_for<N>(active)), BLOCK, 0, st>>>(S, A, H, active,
-                                                                                                              counters);
+                        for (int k = 0; k < BATCH; ++k)
+                        {
+                                enqueue_iteration(S, P, accum, counters, total_paths, parity, st, times, nullptr);
+                                parity ^= 1;
+                        }
                 }
-                if (timing)
+                e = cudaMemcpyAsync(host_counters, counters, C_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
+                if (e == cudaSuccess)
                 {
-                        cudaEventRecord(ev[2], st);
+                        e = cudaStreamSynchronize(st);
                 }
-                cudaMemsetAsync(counters + C_ACTIVE_OUT, 0, 2 * sizeof(unsigned long long), st);
-                cudaMemsetAsync(counters + C_SMOOTH, 0, sizeof(unsigned long long), st);
-                long long shade_blocks = std::min<long long>(grid_for<N>(active), 148LL * 16);
-                if (S.smooth_normal && !sm_f)
+                if (e != cudaSuccess || host_counters[C_DONE] || host_counters[C_ERROR])
                 {
-                        return cudaErrorInvalidValue;  // the pool was carved without the smooth-normal queue
+                        break;
                 }
-                k_shade<N><<<(unsigned)shade_blocks, BLOCK, 0, st>>>(S, P, A, H, B, SQ, SM, accum, active, counters);
-                if (timing)
-                {
-                        cudaEventRecord(ev[3], st);
-                }
-                cudaMemcpyAsync(host_counters, counters, C_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st);
-                cudaError_t e = cudaStreamSynchronize(st);
-                if (e != cudaSuccess)
-                {
-                        return e;
-                }
-                long long survivors = (long long)host_counters[C_ACTIVE_OUT];
-                long long shadows = (long long)host_counters[C_SHADOW];
-                long long smooth_rays = (long long)host_counters[C_SMOOTH];
-                if (smooth_rays > 0)
-                {
-                        k_shadow_smooth<N><<<(unsigned)grid_for<N>(smooth_rays), BLOCK, 0, st>>>(S, SM, accum, smooth_rays,
-                                                                                                   counters);
-                        times->launches += 1;
-                }
-                if (shadows > 0 && one_mesh)
-                {
-                        k_shadow_refill<N><<<(unsigned)std::min(shadow_refill_blocks, grid_for<N>(shadows)), BLOCK, 0, st>>>(
-                                S, SQ, accum, shadows, counters);
-                }
-                else if (shadows > 0)
-                {
-                        k_shadow<N><<<(unsigned)std::min(shadow_blocks, grid_for<N>(shadows)), BLOCK, 0, st>>>(
-                                S, SQ, accum, shadows, counters);
-                }
-                if (timing)
-                {
-                        cudaEventRecord(ev[4], st);
-                        cudaEventSynchronize(ev[4]);
-                        float ms;
-                        cudaEventElapsedTime(&ms, ev[0], ev[1]);
-                        times->raygen_ms += ms;
-                        cudaEventElapsedTime(&ms, ev[1], ev[2]);
-                        times->extend_ms += ms;
-                        cudaEventElapsedTime(&ms, ev[2], ev[3]);
-                        times->shade_ms += ms;
-                        cudaEventElapsedTime(&ms, ev[3], ev[4]);
-                        times->shadow_ms += ms;
-                }
-                times->extend_launches += 1;
-                times->shadow_launches += shadows > 0 ? 1 : 0;
-                times->launches += (fresh > 0 ? 1 : 0) + 2 + (shadows > 0 ? 1 : 0);
-                times->extend_rays += active;
-                times->shadow_rays += shadows;
-                active = survivors;
-                flip = !flip;
+        }
+        if (exec)
+        {
+                cudaGraphExecDestroy(exec);
         }
         if (timing)
         {
-                for (auto& e : ev)
+                for (auto& v : ev)
                 {
-                        cudaEventDestroy(e);
+                        cudaEventDestroy(v);
                 }
+        }
+        if (e != cudaSuccess)
+        {
+                return e;
         }
         return cudaGetLastError();
 }

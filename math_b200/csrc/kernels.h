@@ -52,12 +52,26 @@ struct Wavefront
         void carve(char* base, long long Q, int lights, bool smooth = false);
 
         // Traces total_paths camera paths starting at P.path_begin into accum (3 doubles per pixel).
-        // counters: C_COUNT device int64; host_counters: pinned host mirror of the first two.
+        // counters: C_COUNT device int64 (work counters and the wavefront control); host_counters:
+        // pinned host mirror of all of them.
         // times: launch counts always, per-kernel device times when timing (events around every
         // launch); stop: optional host flag polled once per wavefront iteration (between launches).
+        // The iterations run in batches of `batch` captured as one CUDA graph (use_graph; else enqueued
+        // directly), the host reading the done flag after each batch.
         cudaError_t run(const DevScene<N>& S, PassDev P, double* accum, unsigned long long* counters,
                         unsigned long long* host_counters, long long total_paths, cudaStream_t st, KernelTimes* times,
-                        bool timing, const volatile int* stop);
+                        bool timing, const volatile int* stop, bool use_graph = true, int batch = 4);
+
+        // One wavefront iteration on stream st (k_iter_begin .. k_iter_end; the queue sizes live in
+        // counters, so nothing waits for the host).  parity selects which double-buffered queue is
+        // current; ev (6 events, optional) are recorded around the kernel kinds.  Capturable.
+        void enqueue_iteration(const DevScene<N>& S, const PassDev& P, double* accum, unsigned long long* counters,
+                               long long total_paths, int parity, cudaStream_t st, KernelTimes* times,
+                               cudaEvent_t* ev) const;
+        static int iteration_launches(bool smooth)
+        {
+                return 6 + (smooth ? 1 : 0);
+        }
 };
 
 // Denoiser inputs: first-hit normal and depth of every pixel-centre camera ray; per-pixel mean and

@@ -1264,12 +1264,50 @@ bool smooth_shading(const nt_scene* s, const nt_render_opts& o)
         return false;
 }
 
-// One pass of samples_per_pixel; moments_accum: per-path sums (pixel * spp_eff + sample, 3 doubles
-// each, zeroed by the caller) instead of the scene's per-pixel accumulator (nt_render_moments).
-template <int N>
-void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_accum = nullptr)
+// A pass of one scene prepared for the wavefront: checks, the pass constants, the path pool.  Type-
+// erased over N so that passes of scenes of different dimensions can run side by side
+// (nt_render_batch).
+struct PassJob
 {
-        auto t0 = std::chrono::steady_clock::now();
+        nt_scene* s = nullptr;
+        long long total = 0;
+        long long spp_eff = 0;
+        bool smooth = false;
+        KernelTimes times;
+        std::chrono::steady_clock::time_point t0;
+        virtual ~PassJob() = default;
+        // one wavefront iteration of this pass on stream st
+        virtual void enqueue(int parity, cudaStream_t st) = 0;
+        // the whole pass on the scene's stream
+        virtual cudaError_t run(const nt_render_opts& o) = 0;
+};
+
+template <int N>
+struct PassJobN final : PassJob
+{
+        DevScene<N> S;
+        PassDev P{};
+        Wavefront<N> W;
+        double* accum = nullptr;
+        void enqueue(int parity, cudaStream_t st) override
+        {
+                W.enqueue_iteration(S, P, accum, s->counters.as<unsigned long long>(), total, parity, st, nullptr, nullptr);
+        }
+        cudaError_t run(const nt_render_opts& o) override
+        {
+                return W.run(S, P, accum, s->counters.as<unsigned long long>(), s->host_counters, total, s->stream, &times,
+                             o.timing != 0, o.stop, true, o.graph_iterations > 0 ? o.graph_iterations : 4);
+        }
+};
+
+// moments_accum: per-path sums (pixel * spp_eff + sample, 3 doubles each, zeroed by the caller)
+// instead of the scene's per-pixel accumulator (nt_render_moments).
+template <int N>
+std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, double* moments_accum)
+{
+        auto job = std::make_unique<PassJobN<N>>();
+        job->t0 = std::chrono::steady_clock::now();
+        job->s = s;
         if (o.samples_per_pixel < 1)
         {
                 fail(NT_EINVAL, "Stratified jittered sample count is not a positive integer");
@@ -1284,7 +1322,7 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
         {
                 spp_eff *= k;
         }
-        DevScene<N> S;
+        DevScene<N>& S = job->S;
         std::memcpy(&S, s->dev_scene.data(), sizeof(S));
         S.max_depth = o.max_depth;
         S.retest = o.retest;
@@ -1309,10 +1347,10 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
                 s->pool_lights = lights;
                 s->pool_smooth = smooth;
         }
-        Wavefront<N> W;
-        W.carve(s->pool.as<char>(), s->pool_paths, s->pool_lights, smooth);
+        // the pool may be larger than this pass asks for: carve the pass's Q from it
+        job->W.carve(s->pool.as<char>(), Q, s->pool_lights, smooth);
 
-        PassDev P{};
+        PassDev& P = job->P;
         P.key0 = (uint32_t)o.seed;
         P.key1 = (uint32_t)(o.seed >> 32);
         P.spp_eff = (int)spp_eff;
@@ -1327,21 +1365,32 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
         {
                 fail(NT_EINVAL, "too many paths in one moments pass");
         }
+        job->accum = moments_accum ? moments_accum : s->accum.as<double>();
+        job->total = total;
+        job->spp_eff = spp_eff;
+        job->smooth = smooth;
         check_cuda(cudaMemsetAsync(s->counters.p, 0, s->counters.bytes, s->stream), "memset counters");
-        KernelTimes times;
-        cudaError_t e = W.run(S, P, moments_accum ? moments_accum : s->accum.as<double>(), s->counters.as<unsigned long long>(),
-                              s->host_counters, total, s->stream, &times, o.timing != 0, o.stop);
-        check_cuda(e, "render");
-        check_cuda(cudaMemcpyAsync(s->host_counters, s->counters.p, C_COUNT * sizeof(unsigned long long),
-                                   cudaMemcpyDeviceToHost, s->stream),
-                   "counters");
+        return job;
+}
+
+// After a pass: counters to the host (already there after a batch), statistics, state.
+void finish_pass(PassJob& job, const nt_render_opts& o, nt_stats* st, bool copy_counters)
+{
+        nt_scene* s = job.s;
+        if (copy_counters)
+        {
+                check_cuda(cudaMemcpyAsync(s->host_counters, s->counters.p, C_COUNT * sizeof(unsigned long long),
+                                           cudaMemcpyDeviceToHost, s->stream),
+                           "counters");
+        }
         check_cuda(cudaStreamSynchronize(s->stream), "render sync");
-        bool stopped = o.stop && *o.stop;
-        s->samples_done += stopped ? 0 : spp_eff;
+        const bool stopped = (o.stop && *o.stop) || !s->host_counters[C_DONE];
+        s->samples_done += stopped ? 0 : job.spp_eff;
         if (st)
         {
+                const KernelTimes& times = job.times;
                 std::memset(st, 0, sizeof(*st));
-                st->paths = total;
+                st->paths = job.total;
                 st->rays = (int64_t)s->host_counters[C_RAYS];
                 st->shadow_rays = (int64_t)s->host_counters[C_SHADOW_RAYS];
                 st->facet_tests = (int64_t)s->host_counters[C_FACET_TESTS];
@@ -1349,7 +1398,7 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
                 st->retests = (int64_t)s->host_counters[C_RETESTS];
                 st->descent_levels = (int64_t)s->host_counters[C_DESCENT];
                 st->error_bits = (int64_t)s->host_counters[C_ERROR];
-                st->spp_effective = (int)spp_eff;
+                st->spp_effective = (int)job.spp_eff;
                 st->raygen_ms = times.raygen_ms;
                 st->extend_ms = times.extend_ms;
                 st->shade_ms = times.shade_ms;
@@ -1361,16 +1410,25 @@ void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_
                 st->shadow_box_steps = (int64_t)s->host_counters[C_SH_BOX_STEPS];
                 st->shadow_retests = (int64_t)s->host_counters[C_SH_RETESTS];
                 st->shadow_descent_levels = (int64_t)s->host_counters[C_SH_DESCENT];
-                st->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
-        }
-        if (stopped)
-        {
-                fail(NT_ESTOPPED, "render stopped");
+                st->iterations = (int64_t)s->host_counters[C_ITERS];
+                st->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - job.t0).count();
         }
         if (s->host_counters[C_ERROR])
         {
                 fail(NT_ETIMEOUT, "a bounded device loop ran out (error bits " + std::to_string(s->host_counters[C_ERROR]) + ")");
         }
+        if (stopped)
+        {
+                fail(NT_ESTOPPED, "render stopped");
+        }
+}
+
+template <int N>
+void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_accum = nullptr)
+{
+        std::unique_ptr<PassJob> job = prepare_pass<N>(s, o, moments_accum);
+        check_cuda(job->run(o), "render");
+        finish_pass(*job, o, st, true);
 }
 
 // One pass of the wavefront on caller-provided working memory (nt_render_noalloc): the scratch holds
@@ -1449,7 +1507,8 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
         check_cuda(cudaMemsetAsync(counters, 0, C_COUNT * sizeof(unsigned long long), st), "memset counters");
         unsigned long long host_counters[C_COUNT] = {};
         KernelTimes times;
-        check_cuda(W.run(S, P, d_accum, counters, host_counters, total, st, &times, false, o.stop), "render");
+        // enqueued directly: a graph instantiation may allocate, and the caller's stream may be capturing
+        check_cuda(W.run(S, P, d_accum, counters, host_counters, total, st, &times, false, o.stop, false), "render");
         check_cuda(cudaMemcpyAsync(host_counters, counters, C_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
                    "counters");
         check_cuda(cudaStreamSynchronize(st), "render sync");
@@ -1539,6 +1598,14 @@ struct RenderF
         static void run(nt_scene* s, const nt_render_opts& o, nt_stats* st)
         {
                 render<N>(s, o, st);
+        }
+};
+template <int N>
+struct PrepareF
+{
+        static void run(nt_scene* s, const nt_render_opts& o, std::unique_ptr<PassJob>* out)
+        {
+                *out = prepare_pass<N>(s, o, nullptr);
         }
 };
 template <int N>
@@ -2109,6 +2176,186 @@ int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int64_t sampl
                 if (stats)
                 {
                         *stats = one;
+                }
+        });
+}
+
+int nt_render_batch(nt_scene* const* scenes, int count, const nt_render_opts* opts, nt_stats* stats)
+{
+        cudaStream_t master = nullptr;
+        std::vector<cudaEvent_t> events;
+        cudaGraphExec_t exec = nullptr;
+        auto cleanup = [&]() {
+                if (exec)
+                {
+                        cudaGraphExecDestroy(exec);
+                }
+                for (cudaEvent_t e : events)
+                {
+                        cudaEventDestroy(e);
+                }
+                if (master)
+                {
+                        cudaStreamDestroy(master);
+                }
+        };
+        int rc = guarded([&]() {
+                if (count < 1 || !scenes || !opts)
+                {
+                        fail(NT_EINVAL, "bad batch arguments");
+                }
+                for (int i = 0; i < count; ++i)
+                {
+                        need_built(scenes[i]);
+                        for (int j = 0; j < i; ++j)
+                        {
+                                if (scenes[j] == scenes[i])
+                                {
+                                        fail(NT_EINVAL, "a scene appears twice in the batch");
+                                }
+                        }
+                }
+                std::vector<std::unique_ptr<PassJob>> jobs(count);
+                for (int i = 0; i < count; ++i)
+                {
+                        dispatch<PrepareF>(scenes[i]->n, scenes[i], opts[i], &jobs[i]);
+                }
+                for (int i = 0; i < count; ++i)
+                {
+                        check_cuda(cudaStreamSynchronize(scenes[i]->stream), "batch sync");
+                }
+                // one graph: fork from a master stream to every scene's stream, `per` iterations of
+                // each pass, its counters to the host, join back
+                const int batch = opts[0].graph_iterations > 0 ? opts[0].graph_iterations : 4;
+                const int per = batch + (batch & 1);
+                check_cuda(cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking), "cudaStreamCreate");
+                events.resize(count + 1);
+                for (cudaEvent_t& e : events)
+                {
+                        check_cuda(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+                }
+                check_cuda(cudaStreamBeginCapture(master, cudaStreamCaptureModeThreadLocal), "capture");
+                cudaGraph_t graph = nullptr;
+                cudaError_t e = cudaEventRecord(events[count], master);
+                for (int i = 0; i < count && e == cudaSuccess; ++i)
+                {
+                        nt_scene* s = scenes[i];
+                        e = cudaStreamWaitEvent(s->stream, events[count], 0);
+                        for (int k = 0; k < per && e == cudaSuccess; ++k)
+                        {
+                                jobs[i]->enqueue(k & 1, s->stream);
+                        }
+                        if (e == cudaSuccess)
+                        {
+                                e = cudaMemcpyAsync(s->host_counters, s->counters.p, C_COUNT * sizeof(unsigned long long),
+                                                    cudaMemcpyDeviceToHost, s->stream);
+                        }
+                        if (e == cudaSuccess)
+                        {
+                                e = cudaEventRecord(events[i], s->stream);
+                        }
+                        if (e == cudaSuccess)
+                        {
+                                e = cudaStreamWaitEvent(master, events[i], 0);
+                        }
+                }
+                cudaError_t e2 = cudaStreamEndCapture(master, &graph);
+                check_cuda(e != cudaSuccess ? e : e2, "batch capture");
+                e = cudaGraphInstantiate(&exec, graph, 0);
+                cudaGraphDestroy(graph);
+                check_cuda(e, "batch graph");
+                for (int i = 0; i < count; ++i)
+                {
+                        for (int c = C_Q_ACTIVE; c < C_COUNT; ++c)
+                        {
+                                scenes[i]->host_counters[c] = 0;
+                        }
+                }
+                const volatile int* stop = opts[0].stop;
+                while (true)
+                {
+                        if (stop && *stop)
+                        {
+                                break;
+                        }
+                        check_cuda(cudaGraphLaunch(exec, master), "batch launch");
+                        check_cuda(cudaStreamSynchronize(master), "batch sync");
+                        bool all = true, err = false;
+                        for (int i = 0; i < count; ++i)
+                        {
+                                all &= scenes[i]->host_counters[C_DONE] != 0;
+                                err |= scenes[i]->host_counters[C_ERROR] != 0;
+                                jobs[i]->times.launches += (long long)per * Wavefront<3>::iteration_launches(jobs[i]->smooth);
+                                jobs[i]->times.extend_launches += per;
+                                jobs[i]->times.shadow_launches += per;
+                        }
+                        if (all || err)
+                        {
+                                break;
+                        }
+                }
+                for (int i = 0; i < count; ++i)
+                {
+                        finish_pass(*jobs[i], opts[i], stats ? stats + i : nullptr, false);
+                }
+        });
+        cleanup();
+        return rc;
+}
+
+int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tuned, double* best_ms)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!base || !tuned)
+                {
+                        fail(NT_EINVAL, "null options");
+                }
+                const long long total = scene->pixel_count() * (long long)nt_effective_spp(scene->n, base->samples_per_pixel);
+                std::vector<long long> pools;
+                for (long long q = 1ll << 20; q <= (1ll << 23); q <<= 1)
+                {
+                        if (q < 2 * total || pools.empty())
+                        {
+                                pools.push_back(std::min(q, std::max<long long>(256, total)));
+                        }
+                }
+                const int iters[] = {2, 4, 8};
+                nt_render_opts best = *base;
+                double best_t = 1e300;
+                for (long long q : pools)
+                {
+                        for (int it : iters)
+                        {
+                                nt_render_opts o = *base;
+                                o.pool_paths = q;
+                                o.graph_iterations = it;
+                                o.timing = 0;
+                                o.stop = nullptr;
+                                // one warm pass, one timed
+                                for (int rep = 0; rep < 2; ++rep)
+                                {
+                                        auto t0 = std::chrono::steady_clock::now();
+                                        dispatch<RenderF>(scene->n, scene, o, (nt_stats*)nullptr);
+                                        const double ms =
+                                                std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                                        if (rep == 1 && ms < best_t)
+                                        {
+                                                best_t = ms;
+                                                best = o;
+                                        }
+                                }
+                        }
+                }
+                check_cuda(cudaMemsetAsync(scene->accum.p, 0, scene->accum.bytes, scene->stream), "memset");
+                check_cuda(cudaStreamSynchronize(scene->stream), "sync");
+                scene->samples_done = 0;
+                best.timing = base->timing;
+                best.stop = base->stop;
+                *tuned = best;
+                if (best_ms)
+                {
+                        *best_ms = best_t;
                 }
         });
 }

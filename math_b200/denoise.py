@@ -275,14 +275,15 @@ def render_reference(scene: ntrace.Scene, spp: int, seed: int, max_depth: int = 
 
 
 def make_pairs(scene: ntrace.Scene, count: int, seed: int, screen: int, spp_in: int, spp_ref: int,
-               max_depth: int = 5, has_floor: bool = True, units_per_pixel: float | None = None) -> list[dict]:
+               max_depth: int = 5, has_floor: bool = True, units_per_pixel: float | None = None,
+               extent: float = 8.0) -> list[dict]:
     """`count` training pairs from seeded variations of `scene`: spp_in samples per pixel (the noisy
     input with its moments) and spp_ref samples (the target), both stratified."""
     n = scene.n
     rng = np.random.default_rng(seed)
     pairs = []
     for i in range(count):
-        v = random_variant(n, rng, screen, units_per_pixel=units_per_pixel)
+        v = random_variant(n, rng, screen, extent=extent, units_per_pixel=units_per_pixel)
         apply_variant(scene, v, has_floor)
         x = render_inputs(scene, spp_in, seed=seed * 100003 + 2 * i, max_depth=max_depth)
         x["target"] = render_reference(scene, spp_ref, seed=seed * 100003 + 2 * i + 1, max_depth=max_depth)

@@ -33,7 +33,8 @@ EXPORTED_SYMBOLS = (
     "nt_scene_set_projector", "nt_scene_set_background", "nt_scene_build", "nt_scene_mesh_info", "nt_render",
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
-    "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_clear_lights", "nt_scene_set_object_surface", "nt_render_aux",
+    "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_clear_lights", "nt_render_batch",
+    "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
     "nt_render_moments", "nt_render_noalloc",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
     "nt_denoiser_set_params", "nt_denoiser_set_input", "nt_denoiser_apply", "nt_denoiser_gradient",
@@ -59,7 +60,7 @@ class BuildOpts(ctypes.Structure):
 class RenderOpts(ctypes.Structure):
     _fields_ = [("samples_per_pixel", ctypes.c_int), ("max_depth", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("retest", ctypes.c_int), ("smooth_normal", ctypes.c_int), ("pool_paths", ctypes.c_int64),
-                ("timing", ctypes.c_int), ("stop", ctypes.c_void_p)]
+                ("timing", ctypes.c_int), ("stop", ctypes.c_void_p), ("graph_iterations", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -70,7 +71,8 @@ class Stats(ctypes.Structure):
                 ("shade_ms", ctypes.c_double), ("shadow_ms", ctypes.c_double), ("launches", ctypes.c_int64),
                 ("extend_launches", ctypes.c_int64), ("shadow_launches", ctypes.c_int64),
                 ("shadow_facet_tests", ctypes.c_int64), ("shadow_box_steps", ctypes.c_int64),
-                ("shadow_retests", ctypes.c_int64), ("shadow_descent_levels", ctypes.c_int64)]
+                ("shadow_retests", ctypes.c_int64), ("shadow_descent_levels", ctypes.c_int64),
+                ("iterations", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
@@ -132,6 +134,10 @@ def library() -> ctypes.CDLL:
         "nt_cosine_sphere_coefficient": ([ctypes.c_int], ctypes.c_double),
         "nt_scene_set_mesh_normals": ([vp, ctypes.c_int, f32p, i64, i32p], ctypes.c_int),
         "nt_scene_clear_lights": ([vp], ctypes.c_int),
+        "nt_render_batch": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(RenderOpts), ctypes.POINTER(Stats)],
+                            ctypes.c_int),
+        "nt_autotune": ([vp, ctypes.POINTER(RenderOpts), ctypes.POINTER(RenderOpts), ctypes.POINTER(ctypes.c_double)],
+                        ctypes.c_int),
         "nt_scene_set_object_surface": ([vp, ctypes.c_int, ctypes.POINTER(Surface)], ctypes.c_int),
         "nt_render_aux": ([vp, vp, vp, vp], ctypes.c_int),
         "nt_render_moments": ([vp, ctypes.POINTER(RenderOpts), i64, vp, vp, ctypes.POINTER(Stats)], ctypes.c_int),
@@ -173,6 +179,25 @@ def effective_spp(n: int, spp: int) -> int:
 
 def cosine_sphere_coefficient(n: int) -> float:
     return library().nt_cosine_sphere_coefficient(n)
+
+
+def render_opts(samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
+                smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False,
+                graph_iterations: int = 0) -> RenderOpts:
+    return RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)),
+                      int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None, int(graph_iterations))
+
+
+def render_batch(scenes: list, opts: list[dict]) -> list[dict]:
+    """One pass of each scene, run side by side in one CUDA graph (nt_render_batch); opts[i] holds
+    the keyword arguments of Scene.render for scene i."""
+    lib = library()
+    n = len(scenes)
+    handles = (ctypes.c_void_p * n)(*[sc._h.value for sc in scenes])
+    arr = (RenderOpts * n)(*[render_opts(**o) for o in opts])
+    st = (Stats * n)()
+    _check(lib.nt_render_batch(handles, n, arr, st))
+    return [st[i].as_dict() for i in range(n)]
 
 
 class Scene:
@@ -287,14 +312,25 @@ class Scene:
         return int(b.value)
 
     def render(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
-               smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None) -> dict:
-        o = RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)),
-                       int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None)
+               smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None,
+               graph_iterations: int = 0) -> dict:
+        o = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, pool_paths, timing,
+                        graph_iterations)
         if stop is not None:
             o.stop = ctypes.cast(stop, ctypes.c_void_p)
         st = Stats()
         _check(self._lib.nt_render(self._h, ctypes.byref(o), ctypes.byref(st)))
         return st.as_dict()
+
+    def autotune(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
+                 smooth_normal: bool = False) -> tuple[dict, float]:
+        """Fastest pool size and iterations per graph launch for passes of samples_per_pixel (probe
+        passes; clears the accumulator).  Returns ({pool_paths, graph_iterations}, pass ms)."""
+        base = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, 0, False, 0)
+        out = RenderOpts()
+        ms = ctypes.c_double()
+        _check(self._lib.nt_autotune(self._h, ctypes.byref(base), ctypes.byref(out), ctypes.byref(ms)))
+        return {"pool_paths": int(out.pool_paths), "graph_iterations": int(out.graph_iterations)}, float(ms.value)
 
     def clear(self) -> None:
         _check(self._lib.nt_accum_clear(self._h))

@@ -9,10 +9,11 @@ mean and variance of the mean), plus the first-hit normal and depth; the target 
 render.  The input sample count of each pair is drawn from --spp-in, so one
 network covers several noise levels.  Weights go to <out>/denoiser_n<n>.npz.
 
-Evaluation (--eval): a held-out variation on a larger screen; the reference is a 64k-sample render
-(effective k^(n-1) >= 65536); plain renders at 1, 4, 16, ... samples and denoised renders of the
-inputs at each --spp-in give (time, relative RMSE) points; the report is the time each method needs
-to reach --target (the smallest measured spp that reaches it).
+Evaluation (--eval): a held-out variation at the measured configuration's screen size (400^2, 128^3,
+48^4); plain renders at 1, 4, 16, ... samples and denoised renders at each --spp-in, timed over the
+whole frame, give (time, relative RMSE) points, the error measured on the centred window (128^2,
+32^3, 16^4) against a 64k-sample render of that window (effective k^(n-1) >= 65536); the report is
+the time each method needs to reach --target.
 """
 
 from __future__ import annotations
@@ -27,9 +28,11 @@ import numpy as np
 
 from . import denoise, ntrace, scenes
 
-TRAIN_SCREEN = {3: 64, 4: 24, 5: 10, 6: 6}   # training crops, at the evaluation screen's pixel scale
-EVAL_SCREEN = {3: 256, 4: 48, 5: 16, 6: 8}    # evaluation: the whole 8 x ... x 8 view
+TRAIN_SCREEN = {3: 64, 4: 24, 5: 10, 6: 6}    # training crops, at the measured screen's pixel scale
+EVAL_SCREEN = {3: 400, 4: 128, 5: 48, 6: 16}   # the measured configurations' screens over the 8 x ... x 8 view
+REF_CROP = {3: 128, 4: 32, 5: 16, 6: 8}        # centred window rendered at 64k samples as the reference
 EXTENT = 8.0
+CROP_EXTENT = 4.0                              # training crops lie inside the central 4 x ... x 4 region
 REF_SPP = 65536
 
 
@@ -56,21 +59,32 @@ def make_mixed_pairs(scene, n: int, count: int, seed: int, spp_in: list[int], sp
     for i in range(count):
         s = int(spp_in[rng.integers(len(spp_in))])
         pairs += denoise.make_pairs(scene, 1, seed=seed * 7919 + i, screen=TRAIN_SCREEN[n], spp_in=s, spp_ref=spp_ref,
-                                    units_per_pixel=EXTENT / EVAL_SCREEN[n])
+                                    units_per_pixel=EXTENT / EVAL_SCREEN[n], extent=CROP_EXTENT)
     return pairs
 
 
-def time_to_rmse(scene, den, n: int, screen: int, spp_in: list[int], target: float, seed: int,
-                 max_plain_spp: int = 1 << 14) -> dict:
-    """(time, RMSE) of plain and denoised renders of one held-out variation against a 64k render."""
+def crop(img, n: int, full: int, size: int):
+    """The centred size^(n-1) window of a full^(n-1) image (pixels x0 fastest)."""
+    a = np.asarray(img.detach().cpu() if hasattr(img, "detach") else img).reshape([full] * (n - 1) + [3])
+    o = (full - size) // 2
+    return a[tuple([slice(o, o + size)] * (n - 1))].reshape(-1, 3)
+
+
+def time_to_rmse(scene, den, n: int, spp_in: list[int], target: float, seed: int, max_plain_spp: int = 1 << 12) -> dict:
+    """Plain and denoised renders of one held-out variation at the measured screen size, timed over
+    the whole frame; their error is measured on the centred window against a 64k-sample render of
+    that window (same pixel grid)."""
     import torch
 
+    full, size = EVAL_SCREEN[n], REF_CROP[n]
     rng = np.random.default_rng(seed)
-    v = denoise.random_variant(n, rng, screen)
-    denoise.apply_variant(scene, v)
+    v = denoise.random_variant(n, rng, full)
+    w = dict(v, screen=[size] * (n - 1))
+    denoise.apply_variant(scene, w)
     t0 = time.perf_counter()
-    ref = denoise.render_reference(scene, REF_SPP, seed=seed + 1)
+    ref = denoise.render_reference(scene, REF_SPP, seed=seed + 1).cpu().numpy()
     ref_s = time.perf_counter() - t0
+    denoise.apply_variant(scene, v)
     plain = []
     spp = 1
     while spp <= max_plain_spp:
@@ -79,13 +93,14 @@ def time_to_rmse(scene, den, n: int, screen: int, spp_in: list[int], target: flo
         scene.render(spp, max_depth=5, seed=seed + 2 + spp)
         dt = time.perf_counter() - t0
         img, _ = scene.image()
-        plain.append({"spp": ntrace.effective_spp(n, spp), "seconds": dt, "rmse": denoise.relative_rmse(img, ref)})
+        plain.append({"spp": ntrace.effective_spp(n, spp), "seconds": dt,
+                      "rmse": denoise.relative_rmse(crop(img, n, full, size), ref)})
         if plain[-1]["rmse"] <= target:
             break
         spp *= 4
     den_pts = []
     for s in spp_in:
-        # warm (allocations of the denoiser's workspace happen on first use)
+        # warm (the denoiser's workspace is allocated on first use)
         x = denoise.render_inputs(scene, s, seed=seed + 5)
         den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
         den.apply()
@@ -96,16 +111,18 @@ def time_to_rmse(scene, den, n: int, screen: int, spp_in: list[int], target: flo
         out = den.apply()
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
-        den_pts.append({"spp": ntrace.effective_spp(n, s), "seconds": dt, "rmse": denoise.relative_rmse(out, ref),
-                        "input_rmse": denoise.relative_rmse(x["mean"], ref)})
+        den_pts.append({"spp": ntrace.effective_spp(n, s), "seconds": dt,
+                        "rmse": denoise.relative_rmse(crop(out, n, full, size), ref),
+                        "input_rmse": denoise.relative_rmse(crop(x["mean"], n, full, size), ref)})
 
     def first(points):
         ok = [p for p in points if p["rmse"] <= target]
         return min(ok, key=lambda p: p["seconds"]) if ok else None
 
     bp, bd = first(plain), first(den_pts)
-    return {"n": n, "screen": [screen] * (n - 1), "reference_spp": ntrace.effective_spp(n, REF_SPP),
-            "reference_seconds": ref_s, "target_rmse": target, "plain": plain, "denoised": den_pts,
+    return {"n": n, "screen": [full] * (n - 1), "reference_window": [size] * (n - 1),
+            "reference_spp": ntrace.effective_spp(n, REF_SPP), "reference_seconds": ref_s, "target_rmse": target,
+            "plain": plain, "denoised": den_pts,
             "plain_time_to_target": bp["seconds"] if bp else None,
             "denoised_time_to_target": bd["seconds"] if bd else None,
             "speedup": (bp["seconds"] / bd["seconds"]) if (bp and bd) else None}
@@ -155,8 +172,7 @@ def main(argv=None) -> None:
             den.save(path)
             report["weights"] = str(path)
         if args.eval:
-            report["time_to_rmse"] = time_to_rmse(scene, den, n, EVAL_SCREEN[n], args.spp_in, args.target,
-                                                  seed=args.seed + 77 + n)
+            report["time_to_rmse"] = time_to_rmse(scene, den, n, args.spp_in, args.target, seed=args.seed + 77 + n)
         print(json.dumps(report), flush=True)
         scene.close()
 
