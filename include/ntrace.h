@@ -126,12 +126,25 @@ int nt_scene_add_mesh(nt_scene* scene, const float* vertices, int64_t vertex_cou
 
 /* Vertex normals of mesh object `object` (the Obj's normals and per-facet normal indices that
  * MeshHyperplaneSimplex takes, mesh_hyperplane_simplex.cpp:59-143): normals is normal_count x n;
- * facet_normals is facet_count x n indices into normals, or NULL for the facet's vertex indices.  Each
+ * facet_normals is facet_count x n indices into normals (all n of a facet -1: that facet has none and
+ * is flat), or NULL for the facet's vertex indices.  Each
  * facet is classified as the reference does: any |cos(vertex normal, facet normal)| < 0.7 -> flat;
  * all positive -> interpolated; all negative -> interpolated with the facet normal reversed; mixed ->
  * interpolated with the negative ones reversed.  Used when nt_render_opts.smooth_normal is set. */
 int nt_scene_set_mesh_normals(nt_scene* scene, int object, const float* normals, int64_t normal_count,
                               const int32_t* facet_normals);
+
+/* Mesh from an OBJ (n = 3) or OBJ-n (n > 3) file, as the reference's loader reads its geometry
+ * (src/obj/file/file_load.cpp): "v" lines of n coordinates, "vn" lines of n normal components, "f"
+ * lines of vertex[/texture[/normal]] groups (1-based, negative counted back from the end), facets of
+ * more than n groups split into a fan around the first; texture coordinates, materials and other
+ * lines are skipped.  Added as a mesh object with `surface`; its vertex normals (if any facet has
+ * them) as by nt_scene_set_mesh_normals. */
+int nt_scene_add_obj_file(nt_scene* scene, const char* path, const nt_surface* surface);
+
+/* The scene's dimension n, and the number of objects added so far (-1 for a NULL scene). */
+int nt_scene_dimension(nt_scene* scene);
+int nt_scene_object_count(nt_scene* scene);
 
 /* n-parallelotope: VisibleParallelotope(org, e0..e(n-1)) (visible_shapes.h:75-117).  edges: n x n. */
 int nt_scene_add_parallelotope(nt_scene* scene, const float* org, const float* edges, const nt_surface* surface);

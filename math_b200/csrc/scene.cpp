@@ -495,7 +495,7 @@ void build_mesh(MeshHost& m, unsigned threads)
                         }
                         r32[Rec32<N>::OFF_B] = B;
                         r32[Rec32<N>::OFF_D] = D;
-                        if (has_normals)
+                        if (has_normals && m.facet_normals[f * N] >= 0)
                         {
                                 // NormalType (mesh_hyperplane_simplex.cpp:96-143); LIMIT_COSINE = 0.7
                                 double dots[N];
@@ -1820,11 +1820,16 @@ int nt_scene_set_mesh_normals(nt_scene* scene, int object, const float* normals,
                 std::vector<float> nv = vec_copy(normals, (size_t)normal_count * n, "normals");
                 std::vector<int32_t> fn = facet_normals ? std::vector<int32_t>(facet_normals, facet_normals + m.facets.size())
                                                         : m.facets;
-                for (int32_t i : fn)
+                for (size_t f = 0; f < fn.size() / n; ++f)
                 {
-                        if (i < 0 || i >= normal_count)
+                        const bool none = fn[f * n] < 0;
+                        for (int i = 0; i < n; ++i)
                         {
-                                fail(NT_EINVAL, "facet normal index out of range");
+                                const int32_t x = fn[f * n + i];
+                                if (none ? x != -1 : (x < 0 || x >= normal_count))
+                                {
+                                        fail(NT_EINVAL, "facet normal index out of range");
+                                }
                         }
                 }
                 m.normals = std::move(nv);
@@ -1965,6 +1970,16 @@ int nt_scene_set_background(nt_scene* scene, const nt_surface* surface)
                 scene->background = *surface;
                 scene->built = false;
         });
+}
+
+int nt_scene_dimension(nt_scene* scene)
+{
+        return scene ? scene->n : -1;
+}
+
+int nt_scene_object_count(nt_scene* scene)
+{
+        return scene ? (int)scene->objects.size() : -1;
 }
 
 int nt_scene_clear_lights(nt_scene* scene)

@@ -33,7 +33,8 @@ EXPORTED_SYMBOLS = (
     "nt_scene_set_projector", "nt_scene_set_background", "nt_scene_build", "nt_scene_mesh_info", "nt_render",
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
-    "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_clear_lights", "nt_render_batch",
+    "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_add_obj_file", "nt_scene_dimension",
+    "nt_scene_object_count", "nt_scene_clear_lights", "nt_render_batch",
     "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
     "nt_render_moments", "nt_render_noalloc",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
@@ -133,6 +134,9 @@ def library() -> ctypes.CDLL:
         "nt_effective_spp": ([ctypes.c_int, ctypes.c_int], ctypes.c_int),
         "nt_cosine_sphere_coefficient": ([ctypes.c_int], ctypes.c_double),
         "nt_scene_set_mesh_normals": ([vp, ctypes.c_int, f32p, i64, i32p], ctypes.c_int),
+        "nt_scene_add_obj_file": ([vp, ctypes.c_char_p, ctypes.POINTER(Surface)], ctypes.c_int),
+        "nt_scene_dimension": ([vp], ctypes.c_int),
+        "nt_scene_object_count": ([vp], ctypes.c_int),
         "nt_scene_clear_lights": ([vp], ctypes.c_int),
         "nt_render_batch": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(RenderOpts), ctypes.POINTER(Stats)],
                             ctypes.c_int),
@@ -341,6 +345,13 @@ class Scene:
         spp = ctypes.c_int64()
         _check(self._lib.nt_accum_read(self._h, out.ctypes.data, ctypes.byref(spp)))
         return out, int(spp.value)
+
+    def add_obj_file(self, path, color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False,
+                     light_color=(0.0, 0.0, 0.0)) -> int:
+        """Mesh from an OBJ / OBJ-n file; returns its object index."""
+        s = _surface(color, diffuse, light_source, light_color)
+        _check(self._lib.nt_scene_add_obj_file(self._h, str(path).encode(), ctypes.byref(s)))
+        return self._lib.nt_scene_object_count(self._h) - 1
 
     def set_mesh_normals(self, obj: int, normals, facet_normals=None) -> None:
         """Vertex normals of mesh object `obj` (normal_count x n) and optional per-facet normal indices

@@ -222,7 +222,7 @@ public:
                         typename Obj<N>::Facet& fc = m_facets[f];
                         fc.material = -1;
                         fc.has_texcoord = false;
-                        fc.has_normal = true;
+                        fc.has_normal = !(facet_normals && facet_normals[f * N] < 0);
                         for (unsigned i = 0; i < N; ++i)
                         {
                                 fc.vertices[i] = facets[f * N + i];

