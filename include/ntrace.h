@@ -57,6 +57,8 @@ typedef struct nt_build_opts
         int threads;   /* host threads for the tree build; <= 0: all hardware threads */
         int host_only; /* 1: facet setup and tree build only, no device upload (inspection on hosts
                           without a GPU; render and trace calls then fail with NT_ESTATE) */
+        int tree_on_gpu; /* 1: build the 2^n-trees on the GPU (the same trees, box for box, as the host
+                            build; much faster for large meshes and for n >= 5); ignored with host_only */
 } nt_build_opts;
 
 typedef struct nt_render_opts
@@ -246,6 +248,14 @@ int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int64_t sampl
 int nt_accum_read(nt_scene* scene, float* rgb_mean, int64_t* samples_per_pixel);
 
 int64_t nt_scene_pixel_count(nt_scene* scene);
+
+/* Viewer feed: the running mean of one 2-D slice of the screen as the painter window shows it
+ * (PainterWindow::set_pixel and its row order, src/ui/painter_window/painter_window.cpp:120-153; sRGB
+ * conversion rgb_float_to_srgb_uint8, src/com/color/conversion.cpp:35-42,211-230,344-347): screen
+ * axes 0 and 1 span the slice, slice[j] fixes screen axis j + 2 (n - 3 entries; NULL for n = 3), and
+ * out receives width x height words 0x00RRGGBB, row 0 being the screen's last row.  out is device
+ * memory when device_out, else host memory. */
+int nt_accum_read_srgb_slice(nt_scene* scene, const int32_t* slice, uint32_t* out, int device_out);
 
 /* Copies the scene's device arrays again from the pinned host copy the build kept (a scene whose
  * data arrive from the host for every frame); *bytes: host-to-device bytes moved.  No counterpart in

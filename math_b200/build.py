@@ -92,6 +92,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
+    tree = CSRC / "treebuild.cu"
+    tree_obj = BUILD_DIR / "treebuild.o"
+    if force or _stale(tree_obj, [tree] + headers):
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-fmad=false", "--expt-relaxed-constexpr", "-Xcompiler",
+               "-fPIC,-ffp-contract=off", *common, "-c", str(tree), "-o", str(tree_obj)]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
     objload = CSRC / "objload.cpp"
     objload_obj = BUILD_DIR / "objload.o"
     if force or _stale(objload_obj, [objload, INCLUDE / "ntrace.h"]):
@@ -100,9 +108,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
-    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, denoise_obj, objload_obj]):
+    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, denoise_obj, objload_obj, tree_obj]):
         cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj),
-               str(noalloc_obj), str(denoise_obj), str(objload_obj), "-Xlinker", "--no-undefined", "-lpthread"]
+               str(noalloc_obj), str(denoise_obj), str(objload_obj), str(tree_obj), "-Xlinker", "--no-undefined",
+               "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

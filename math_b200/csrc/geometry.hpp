@@ -13,13 +13,29 @@
 #include <cstdint>
 #include <limits>
 
+// The overlap test is also compiled for the device (the GPU tree build): same operations, same order,
+// no contraction, so the device decides every box-simplex pair as the host does.
+#ifdef __CUDACC__
+#define NT_HD __host__ __device__
+#else
+#define NT_HD
+#endif
+
 namespace ntrace
 {
+template <typename T>
+NT_HD inline void swap_values(T& a, T& b)
+{
+        T t = a;
+        a = b;
+        b = t;
+}
+
 template <int N, typename T>
 using Vec = std::array<T, N>;
 
 template <int N, typename T>
-inline T dot(const Vec<N, T>& a, const Vec<N, T>& b)
+NT_HD inline T dot(const Vec<N, T>& a, const Vec<N, T>& b)
 {
         T r = a[0] * b[0];
         for (int i = 1; i < N; ++i)
@@ -30,7 +46,7 @@ inline T dot(const Vec<N, T>& a, const Vec<N, T>& b)
 }
 
 template <int N, typename T>
-inline Vec<N, T> normalize(const Vec<N, T>& a)
+NT_HD inline Vec<N, T> normalize(const Vec<N, T>& a)
 {
         T len = std::sqrt(dot<N, T>(a, a));
         Vec<N, T> r;
@@ -42,13 +58,13 @@ inline Vec<N, T> normalize(const Vec<N, T>& a)
 }
 
 template <typename T>
-inline T smax(T a, T b)
+NT_HD inline T smax(T a, T b)
 {
         return (a < b) ? b : a;
 }
 
 template <typename T>
-inline T smin(T a, T b)
+NT_HD inline T smin(T a, T b)
 {
         return (b < a) ? b : a;
 }
@@ -278,7 +294,7 @@ struct Box
 {
         Vec<N, T> org, size, d1, d2;
 
-        static Box make(const Vec<N, T>& o, const Vec<N, T>& s)
+        NT_HD static Box make(const Vec<N, T>& o, const Vec<N, T>& s)
         {
                 Box b;
                 for (int i = 0; i < N; ++i)
@@ -291,7 +307,7 @@ struct Box
                 return b;
         }
 
-        bool inside(const Vec<N, T>& p) const
+        NT_HD bool inside(const Vec<N, T>& p) const
         {
                 for (int i = 0; i < N; ++i)
                 {
@@ -304,7 +320,7 @@ struct Box
         }
 
         // first/second slab distances (intersect_impl)
-        bool intersect_impl(const Vec<N, T>& org_r, const Vec<N, T>& dir, T* first, T* second) const
+        NT_HD bool intersect_impl(const Vec<N, T>& org_r, const Vec<N, T>& dir, T* first, T* second) const
         {
                 T f_max = std::numeric_limits<T>::lowest();
                 T b_min = std::numeric_limits<T>::max();
@@ -343,7 +359,7 @@ struct Box
                 return true;
         }
 
-        bool intersect(const Vec<N, T>& o, const Vec<N, T>& dir, T* t) const
+        NT_HD bool intersect(const Vec<N, T>& o, const Vec<N, T>& dir, T* t) const
         {
                 T first, second;
                 if (intersect_impl(o, dir, &first, &second))
@@ -354,7 +370,7 @@ struct Box
                 return false;
         }
 
-        Vec<N, T> vertex(int k) const
+        NT_HD Vec<N, T> vertex(int k) const
         {
                 Vec<N, T> v;
                 for (int i = 0; i < N; ++i)
@@ -459,7 +475,7 @@ struct SimplexShape
         }
 
         // HyperplaneSimplexGeometry::intersect with the ray direction normalised from `direction`
-        bool intersect(const Vec<N, T>& org, const Vec<N, T>& dir, T* t) const
+        NT_HD bool intersect(const Vec<N, T>& org, const Vec<N, T>& dir, T* t) const
         {
                 T s = dot<N, T>(normal, dir);
                 if (!(s != 0))
@@ -506,7 +522,7 @@ struct SimplexShape
 
 // CLRS simplex-method feasibility test of a x + b >= 0 (src/numerical/simplex.h:160-441).
 template <int NS, typename T, int M>
-bool lp_feasible(const std::array<Vec<NS, T>, M>& a_in, const std::array<T, M>& b_in)
+NT_HD bool lp_feasible(const std::array<Vec<NS, T>, M>& a_in, const std::array<T, M>& b_in)
 {
         constexpr int N = NS + 1;
         long long max_iter = 1;
@@ -608,7 +624,7 @@ bool lp_feasible(const std::array<Vec<NS, T>, M>& a_in, const std::array<T, M>& 
                 return true;
         }
         pivot(k, 0);
-        std::swap(map_m[k], map_n[0]);
+        swap_values(map_m[k], map_n[0]);
         for (long long iteration = 2;; ++iteration)
         {
                 T max_abs_c = std::fabs(c[0]);
@@ -654,7 +670,7 @@ bool lp_feasible(const std::array<Vec<NS, T>, M>& a_in, const std::array<T, M>& 
                         return false;
                 }
                 pivot(l, e);
-                std::swap(map_m[l], map_n[e]);
+                swap_values(map_m[l], map_n[e]);
         }
         for (int i = 0; i < N; ++i)
         {
@@ -675,7 +691,7 @@ bool lp_feasible(const std::array<Vec<NS, T>, M>& a_in, const std::array<T, M>& 
 
 // shape_intersection(box, simplex, 10 epsilons) (src/painter/space/shape_intersection.h:343-385)
 template <int N, typename T>
-bool box_simplex_overlap(const Box<N, T>& box, const SimplexShape<N, T>& s)
+NT_HD bool box_simplex_overlap(const Box<N, T>& box, const SimplexShape<N, T>& s)
 {
         constexpr int VC = 1 << N;
         for (int i = 0; i < N; ++i)

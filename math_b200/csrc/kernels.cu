@@ -1028,6 +1028,50 @@ __global__ void k_iter_end(unsigned long long* c, long long total)
         c[C_DONE] = (survivors == 0 && (long long)c[C_Q_NEXT] >= total) ? 1ull : 0ull;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Viewer feed: the running mean of a 2-D slice of the screen as 0x00RRGGBB words, as the painter
+// window stores a pixel (PainterWindow::set_pixel, painter_window.cpp:140-153) with
+// rgb_float_to_srgb_uint8 (com/color/conversion.cpp:35-42,211-230,344-347); the window's row order
+// (pixel[1] = height - 1 - y, painter_window.cpp:126-131) puts screen row height - 1 first.
+
+__device__ __forceinline__ unsigned srgb8(float c)
+{
+        float s;
+        if (c >= 1.0f)
+        {
+                s = 1.0f;
+        }
+        else if (c >= 0.0031308f)
+        {
+                s = 1.055f * powf(c, 1.0f / 2.4f) - 0.055f;
+        }
+        else if (c > 0.0f)
+        {
+                s = c * 12.92f;
+        }
+        else
+        {
+                s = 0.0f;
+        }
+        return (unsigned)(unsigned char)(s * 255.0f + 0.5f);
+}
+
+__global__ void k_srgb_slice(const double* __restrict__ accum, double inv_samples, long long base, int width, int height,
+                             long long row_stride, uint32_t* __restrict__ out)
+{
+        const long long count = (long long)width * height;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (long long)gridDim.x * blockDim.x)
+        {
+                const int x = (int)(i % width);
+                const int y = (int)(i / width);
+                const long long p = base + x + (long long)(height - 1 - y) * row_stride;
+                const float r = (float)(accum[p * 3] * inv_samples);
+                const float g = (float)(accum[p * 3 + 1] * inv_samples);
+                const float b = (float)(accum[p * 3 + 2] * inv_samples);
+                out[i] = (srgb8(r) << 16) | (srgb8(g) << 8) | srgb8(b);
+        }
+}
+
 template <int N>
 long long grid_for(long long count)
 {
@@ -1332,6 +1376,20 @@ cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, fl
         {
                 k_moments_reduce<<<g, BLOCK, 0, st>>>(npix, spp, rad, mean, var);
         }
+        return cudaGetLastError();
+}
+
+cudaError_t launch_srgb_slice(const double* accum, long long samples, long long base, int width, int height,
+                              long long row_stride, uint32_t* out, cudaStream_t st)
+{
+        const long long count = (long long)width * height;
+        if (count <= 0)
+        {
+                return cudaSuccess;
+        }
+        const unsigned g = (unsigned)std::min<long long>((count + BLOCK - 1) / BLOCK, 148LL * 32);
+        k_srgb_slice<<<g, BLOCK, 0, st>>>(accum, samples > 0 ? 1.0 / (double)samples : 0.0, base, width, height, row_stride,
+                                          out);
         return cudaGetLastError();
 }
 

@@ -80,6 +80,10 @@ template <int N>
 cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, float* depth, cudaStream_t st);
 cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, float* mean, float* var, cudaStream_t st);
 
+// Viewer feed: width x height words 0x00RRGGBB (sRGB) of the slice whose first pixel is `base`.
+cudaError_t launch_srgb_slice(const double* accum, long long samples, long long base, int width, int height,
+                              long long row_stride, uint32_t* out, cudaStream_t st);
+
 template <int N>
 cudaError_t launch_trace_closest(const MeshDev<N>& M, const float* org, const float* dir, long long nrays, int retest,
                                  int* facet, float* t, unsigned long long* counters, cudaStream_t st);

@@ -5,6 +5,7 @@
 #include "device_types.h"
 #include "geometry.hpp"
 #include "kernels.h"
+#include "treebuild.h"
 
 #include <algorithm>
 #include <atomic>
@@ -362,7 +363,7 @@ using namespace ntrace;
 // Mesh setup and tree build
 
 template <int N>
-void build_mesh(MeshHost& m, unsigned threads)
+void build_mesh(MeshHost& m, unsigned threads, bool tree_on_gpu, cudaStream_t stream)
 {
         using V32 = Vec<N, float>;
         using V64 = Vec<N, double>;
@@ -643,6 +644,20 @@ void build_mesh(MeshHost& m, unsigned threads)
                 }
         }
 
+        if (tree_on_gpu)
+        {
+                TreeResult tr;
+                build_tree_gpu<N>(shapes, mn, m.level_sizes, max_depth, TREE_MIN_OBJECTS_PER_BOX, stream, &tr);
+                if (tr.error != cudaSuccess)
+                {
+                        fail(tr.error == cudaErrorMemoryAllocation ? NT_ENOMEM : NT_ECUDA, "GPU tree build: " + tr.message);
+                }
+                m.nodes.swap(tr.nodes);
+                m.leaf_idx.swap(tr.leaf_idx);
+                m.leaf_count = tr.leaf_count;
+                m.build_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+                return;
+        }
         // breadth-first: level by level; children of a split box are contiguous
         struct Work
         {
@@ -950,7 +965,7 @@ void check_orthogonal(const Vec<N, float>& dir, const std::array<Vec<N, float>, 
 }
 
 template <int N>
-void build_scene(nt_scene* s, unsigned threads, bool host_only)
+void build_scene(nt_scene* s, unsigned threads, bool host_only, bool tree_on_gpu)
 {
         if (s->objects.empty())
         {
@@ -972,7 +987,7 @@ void build_scene(nt_scene* s, unsigned threads, bool host_only)
         {
                 if (!m.ready)
                 {
-                        build_mesh<N>(m, threads);
+                        build_mesh<N>(m, threads, tree_on_gpu && !host_only, s->stream);
                         m.ready = true;
                         m.uploaded = false;
                 }
@@ -1587,9 +1602,9 @@ void dispatch(int n, A&&... a)
 template <int N>
 struct BuildF
 {
-        static void run(nt_scene* s, unsigned threads, bool host_only)
+        static void run(nt_scene* s, unsigned threads, bool host_only, bool tree_on_gpu)
         {
-                build_scene<N>(s, threads, host_only);
+                build_scene<N>(s, threads, host_only, tree_on_gpu);
         }
 };
 template <int N>
@@ -2022,9 +2037,10 @@ int nt_scene_build(nt_scene* scene, const nt_build_opts* opts)
                 need_scene(scene);
                 unsigned threads = (opts && opts->threads > 0) ? (unsigned)opts->threads : hardware_threads();
                 bool host_only = opts && opts->host_only;
+                bool tree_on_gpu = opts && opts->tree_on_gpu;
                 scene->built = false;
                 scene->built_host = false;
-                dispatch<BuildF>(scene->n, scene, threads, host_only);
+                dispatch<BuildF>(scene->n, scene, threads, host_only, tree_on_gpu);
         });
 }
 
@@ -2372,6 +2388,50 @@ int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tun
                 {
                         *best_ms = best_t;
                 }
+        });
+}
+
+int nt_accum_read_srgb_slice(nt_scene* scene, const int32_t* slice, uint32_t* out, int device_out)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!out || (scene->n > 3 && !slice))
+                {
+                        fail(NT_EINVAL, "null argument");
+                }
+                const int width = scene->screen[0];
+                const int height = scene->screen[1];
+                long long base = 0;
+                long long stride = 1;
+                for (int j = 0; j < scene->n - 1; ++j)
+                {
+                        if (j >= 2)
+                        {
+                                const int v = slice[j - 2];
+                                if (v < 0 || v >= scene->screen[j])
+                                {
+                                        fail(NT_EINVAL, "slice position out of the screen");
+                                }
+                                base += (long long)v * stride;
+                        }
+                        stride *= scene->screen[j];
+                }
+                const size_t bytes = (size_t)width * height * sizeof(uint32_t);
+                DevBuf tmp;
+                uint32_t* dst = out;
+                if (!device_out)
+                {
+                        tmp.alloc(bytes);
+                        dst = tmp.as<uint32_t>();
+                }
+                check_cuda(launch_srgb_slice(scene->accum.as<double>(), scene->samples_done, base, width, height, width, dst,
+                                             scene->stream),
+                           "srgb slice");
+                if (!device_out)
+                {
+                        check_cuda(cudaMemcpyAsync(out, dst, bytes, cudaMemcpyDeviceToHost, scene->stream), "copy");
+                }
+                check_cuda(cudaStreamSynchronize(scene->stream), "sync");
         });
 }
 

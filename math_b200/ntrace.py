@@ -34,7 +34,7 @@ EXPORTED_SYMBOLS = (
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
     "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_add_obj_file", "nt_scene_dimension",
-    "nt_scene_object_count", "nt_scene_clear_lights", "nt_render_batch",
+    "nt_scene_object_count", "nt_accum_read_srgb_slice", "nt_scene_clear_lights", "nt_render_batch",
     "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
     "nt_render_moments", "nt_render_noalloc",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
@@ -55,7 +55,7 @@ class Surface(ctypes.Structure):
 
 
 class BuildOpts(ctypes.Structure):
-    _fields_ = [("threads", ctypes.c_int), ("host_only", ctypes.c_int)]
+    _fields_ = [("threads", ctypes.c_int), ("host_only", ctypes.c_int), ("tree_on_gpu", ctypes.c_int)]
 
 
 class RenderOpts(ctypes.Structure):
@@ -136,6 +136,7 @@ def library() -> ctypes.CDLL:
         "nt_scene_set_mesh_normals": ([vp, ctypes.c_int, f32p, i64, i32p], ctypes.c_int),
         "nt_scene_add_obj_file": ([vp, ctypes.c_char_p, ctypes.POINTER(Surface)], ctypes.c_int),
         "nt_scene_dimension": ([vp], ctypes.c_int),
+        "nt_accum_read_srgb_slice": ([vp, i32p, vp, ctypes.c_int], ctypes.c_int),
         "nt_scene_object_count": ([vp], ctypes.c_int),
         "nt_scene_clear_lights": ([vp], ctypes.c_int),
         "nt_render_batch": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(RenderOpts), ctypes.POINTER(Stats)],
@@ -279,8 +280,9 @@ class Scene:
         s = _surface(color, 1.0, light_source, light_color)
         _check(self._lib.nt_scene_set_background(self._h, ctypes.byref(s)))
 
-    def build(self, threads: int = 0, host_only: bool = False) -> None:
-        o = BuildOpts(threads, int(bool(host_only)))
+    def build(self, threads: int = 0, host_only: bool = False, tree_on_gpu: bool = False) -> None:
+        """Facet setup and 2^n-trees (on the GPU with tree_on_gpu), then the upload."""
+        o = BuildOpts(threads, int(bool(host_only)), int(bool(tree_on_gpu)))
         _check(self._lib.nt_scene_build(self._h, ctypes.byref(o)))
 
     # ---- queries ----
@@ -382,6 +384,15 @@ class Scene:
         st = Stats()
         _check(self._lib.nt_render_moments(self._h, ctypes.byref(o), int(sample_offset), d_mean, d_var, ctypes.byref(st)))
         return st.as_dict()
+
+    def srgb_slice(self, slice_pos=()) -> np.ndarray:
+        """The painter window's view of a 2-D slice: (height, width) words 0x00RRGGBB, row 0 the
+        screen's last row; slice_pos fixes screen axes 2.. (n - 3 values)."""
+        sl = np.ascontiguousarray(np.asarray(slice_pos, np.int32))
+        width, height = self.screen[0], self.screen[1]
+        out = np.zeros((height, width), np.uint32)
+        _check(self._lib.nt_accum_read_srgb_slice(self._h, sl.ctypes.data if sl.size else None, out.ctypes.data, 0))
+        return out
 
     def trace_closest(self, org, dirs, mesh_index: int = 0, retest: bool = True):
         """Closest facet per ray (-1 = miss) and distance; plus the call's statistics."""

@@ -152,7 +152,7 @@ def config(name: str) -> dict:
     raise KeyError(name)
 
 
-def build_scene(spec: dict, threads: int = 0) -> ntrace.Scene:
+def build_scene(spec: dict, threads: int = 0, tree_on_gpu: bool = False) -> ntrace.Scene:
     n = spec["n"]
     s = ntrace.Scene(n)
     if spec["verts"] is not None:
@@ -171,5 +171,5 @@ def build_scene(spec: dict, threads: int = 0) -> ntrace.Scene:
     s.set_projector(P["kind"], P["org"], P["dir"], P["axes"], P["param"], P["screen"])
     bg = spec["bg"]
     s.set_background(bg["color"], bg["light"], bg["light_color"])
-    s.build(threads)
+    s.build(threads, tree_on_gpu=tree_on_gpu)
     return s

@@ -265,3 +265,34 @@ def test_full_scene_render_properties(require_gpu):
     # the background (sky) colour is seen where camera rays miss everything: none do here (the floor
     # covers the screen), so every pixel is lit by the light or the sky through bounces
     assert img.mean() > 0.1
+
+
+def _srgb8(c):
+    """rgb_float_to_srgb_uint8 (src/com/color/conversion.cpp:35-42,211-230,344-347) in float32."""
+    c = np.asarray(c, np.float32)
+    s = np.where(c >= 1, np.float32(1),
+                 np.where(c >= np.float32(0.0031308),
+                          np.float32(1.055) * np.power(np.maximum(c, np.float32(1e-30)), np.float32(1 / 2.4)) - np.float32(0.055),
+                          np.where(c > 0, c * np.float32(12.92), np.float32(0))))
+    return (s.astype(np.float32) * np.float32(255) + np.float32(0.5)).astype(np.uint8).astype(np.uint32)
+
+
+@pytest.mark.parametrize("name", ["n3_small", "n4_small"])
+def test_viewer_feed_slice_matches_the_painter_window_conversion(require_gpu, name):
+    from math_b200 import scenes
+
+    spec = scenes.config(name)
+    s = scenes.build_scene(spec)
+    s.render(spec["spp"], max_depth=spec["max_depth"], seed=6)
+    img, _ = s.image()
+    n = spec["n"]
+    screen = spec["projector"]["screen"]
+    pos = [screen[j] // 2 for j in range(2, n - 1)]
+    got = s.srgb_slice(pos)
+    cube = img.reshape(list(screen[::-1]) + [3])  # (x_{n-2}, ..., x1, x0, rgb)
+    sl = cube[tuple(pos[::-1]) + (slice(None), slice(None))] if pos else cube
+    sl = sl[::-1]  # row 0 = last screen row
+    want = (_srgb8(sl[..., 0]) << 16) | (_srgb8(sl[..., 1]) << 8) | _srgb8(sl[..., 2])
+    assert got.shape == want.shape
+    diff = np.abs(((got >> 16) & 255).astype(int) - ((want >> 16) & 255).astype(int))
+    assert diff.max() <= 1 and (got == want).mean() > 0.99
