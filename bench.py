@@ -36,7 +36,8 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 CONFIGS = {"n3": "n3", "n4": "n4", "n5": "n5"}
-METRIC = "paths/s per n (n=4 plain tracer)"
+def metric_name(n: int) -> str:
+    return f"paths/s per n (n={n} plain tracer)"
 
 
 def measured_peaks() -> dict:
@@ -175,7 +176,7 @@ def run_reference(args) -> None:
     sample = (f"per step {count} random pixels of the {'x'.join(map(str, screen))} frame x {spp_eff} spp, "
               f"paint<{n},float>() of the reference with {threads} threads")
     print(json.dumps({
-        "impl": "reference", "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": args.gpus,
+        "impl": "reference", "metric": metric_name(spec["n"]), "value": value, "unit": "paths/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_block(spec, args),
@@ -229,7 +230,7 @@ def main() -> None:
 
     spec = scenes.config(args.config)
     n = spec["n"]
-    scene = scenes.build_scene(spec)
+    scene = scenes.build_scene(spec, tree_on_gpu=True)
     spp, depth = spec["spp"], spec["max_depth"]
     stream = torch.cuda.ExternalStream(scene.stream)
 
@@ -319,7 +320,7 @@ def main() -> None:
     achieved = walks[dom]["achieved"]
 
     result = {
-        "metric": METRIC, "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "metric": metric_name(n), "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_block(spec, args),

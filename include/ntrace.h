@@ -283,6 +283,18 @@ int nt_trace_closest_device(nt_scene* scene, int mesh_index, const float* d_org,
 int nt_scene_tree_export(nt_scene* scene, int mesh_index, int32_t* nodes, int32_t* indices, float* level_sizes,
                          float* root_org);
 
+/* ---- convex hull (the meshes of the measured scenes) ---- */
+
+/* Boundary facets of the convex hull of `count` points in n = 3..6 dimensions, computed exactly as the
+ * reference's integer hull prepares its input (src/geometry/core/convex_hull.cpp:657-707: shuffled with
+ * mt19937_64(count), scaled to integers in [0, 2^30 - 1], duplicates dropped) with exact integer
+ * predicates.  Facets index the input points (n per facet). */
+typedef struct nt_hull nt_hull;
+int nt_convex_hull(int n, const float* points, int64_t count, nt_hull** out);
+int64_t nt_hull_facet_count(nt_hull* hull);
+int nt_hull_facets(nt_hull* hull, int32_t* facets);
+int nt_hull_destroy(nt_hull* hull);
+
 /* ---- misc ---- */
 
 const char* nt_last_error_message(void);

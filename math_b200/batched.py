@@ -55,7 +55,7 @@ def main(argv=None) -> None:
 
     t0 = time.perf_counter()
     specs = make_workload(args.scenes, args.seed)
-    built = [scenes.build_scene(sp) for sp in specs]
+    built = [scenes.build_scene(sp, tree_on_gpu=True) for sp in specs]
     build_s = time.perf_counter() - t0
     # autotune once per dimension on its largest scene; apply to every scene of that dimension
     tuned = {}

@@ -100,6 +100,14 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
+    hull = CSRC / "hull.cpp"
+    hull_obj = BUILD_DIR / "hull.o"
+    if force or _stale(hull_obj, [hull, INCLUDE / "ntrace.h"]):
+        cmd = [nvcc, "-x", "c++", "-Wno-deprecated-gpu-targets", "-O2", "-Xcompiler", "-fPIC", *common, "-c", str(hull),
+               "-o", str(hull_obj)]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
     objload = CSRC / "objload.cpp"
     objload_obj = BUILD_DIR / "objload.o"
     if force or _stale(objload_obj, [objload, INCLUDE / "ntrace.h"]):
@@ -108,10 +116,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
-    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, denoise_obj, objload_obj, tree_obj]):
+    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, denoise_obj, objload_obj, tree_obj, hull_obj]):
         cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj),
-               str(noalloc_obj), str(denoise_obj), str(objload_obj), str(tree_obj), "-Xlinker", "--no-undefined",
-               "-lpthread"]
+               str(noalloc_obj), str(denoise_obj), str(objload_obj), str(tree_obj), str(hull_obj), "-Xlinker",
+               "--no-undefined", "-lpthread"]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

@@ -34,7 +34,8 @@ EXPORTED_SYMBOLS = (
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
     "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_add_obj_file", "nt_scene_dimension",
-    "nt_scene_object_count", "nt_accum_read_srgb_slice", "nt_scene_clear_lights", "nt_render_batch",
+    "nt_scene_object_count", "nt_accum_read_srgb_slice", "nt_convex_hull", "nt_hull_facet_count", "nt_hull_facets",
+    "nt_hull_destroy", "nt_scene_clear_lights", "nt_render_batch",
     "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
     "nt_render_moments", "nt_render_noalloc",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
@@ -137,6 +138,10 @@ def library() -> ctypes.CDLL:
         "nt_scene_add_obj_file": ([vp, ctypes.c_char_p, ctypes.POINTER(Surface)], ctypes.c_int),
         "nt_scene_dimension": ([vp], ctypes.c_int),
         "nt_accum_read_srgb_slice": ([vp, i32p, vp, ctypes.c_int], ctypes.c_int),
+        "nt_convex_hull": ([ctypes.c_int, f32p, i64, ctypes.POINTER(vp)], ctypes.c_int),
+        "nt_hull_facet_count": ([vp], i64),
+        "nt_hull_facets": ([vp, i32p], ctypes.c_int),
+        "nt_hull_destroy": ([vp], ctypes.c_int),
         "nt_scene_object_count": ([vp], ctypes.c_int),
         "nt_scene_clear_lights": ([vp], ctypes.c_int),
         "nt_render_batch": ([ctypes.POINTER(vp), ctypes.c_int, ctypes.POINTER(RenderOpts), ctypes.POINTER(Stats)],
@@ -176,6 +181,21 @@ def _surface(color=(1.0, 1.0, 1.0), diffuse=1.0, light_source=False, light_color
     s.diffuse = float(diffuse)
     s.light_source = int(bool(light_source))
     return s
+
+
+def convex_hull(points) -> np.ndarray:
+    """Boundary facets (point indices, facet_count x n) of the convex hull of points (count x n)."""
+    lib = library()
+    p = _f32(points)
+    n = p.shape[1]
+    h = ctypes.c_void_p()
+    _check(lib.nt_convex_hull(n, p.ctypes.data, len(p), ctypes.byref(h)))
+    try:
+        out = np.zeros((lib.nt_hull_facet_count(h), n), np.int32)
+        _check(lib.nt_hull_facets(h, out.ctypes.data))
+    finally:
+        lib.nt_hull_destroy(h)
+    return out
 
 
 def effective_spp(n: int, spp: int) -> int:

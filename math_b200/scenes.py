@@ -66,11 +66,18 @@ def sphere_points(n: int, count: int, seed: int) -> np.ndarray:
     return p.astype(np.float32)
 
 
-def sphere_hull(n: int, count: int, seed: int, cap: float | None = None) -> tuple[np.ndarray, np.ndarray]:
-    from scipy.spatial import ConvexHull
-
+def sphere_hull(n: int, count: int, seed: int, cap: float | None = None,
+                method: str = "ntrace") -> tuple[np.ndarray, np.ndarray]:
+    """Boundary of the convex hull of `count` seeded points on the unit (n-1)-sphere (the library's
+    exact hull, nt_convex_hull; method="qhull": scipy's Qhull), optionally without the facets whose
+    centroid direction lies within angle `cap` of +x_(n-1)."""
     pts = sphere_points(n, count, seed)
-    facets = ConvexHull(pts.astype(np.float64)).simplices.astype(np.int32)
+    if method == "qhull":
+        from scipy.spatial import ConvexHull
+
+        facets = ConvexHull(pts.astype(np.float64)).simplices.astype(np.int32)
+    else:
+        facets = ntrace.convex_hull(pts)
     if cap is not None:
         centroid = pts[facets].astype(np.float64).mean(axis=1)
         centroid /= np.linalg.norm(centroid, axis=1, keepdims=True)

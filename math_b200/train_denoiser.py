@@ -148,7 +148,7 @@ def main(argv=None) -> None:
     for n in args.n:
         t0 = time.perf_counter()
         spec = mesh_for(n, args.small)
-        scene = scenes.build_scene(spec)
+        scene = scenes.build_scene(spec, tree_on_gpu=True)
         build_s = time.perf_counter() - t0
         path = out / f"denoiser_n{n}.npz"
         report = {"n": n, "scene_build_seconds": build_s}
