@@ -128,6 +128,40 @@ def time_to_rmse(scene, den, n: int, spp_in: list[int], target: float, seed: int
             "speedup": (bp["seconds"] / bd["seconds"]) if (bp and bd) else None}
 
 
+def synthetic(args) -> None:
+    """Training steps on seeded random features (square-ish screen of about --synthetic pixels): the
+    throughput of the network's kernels alone."""
+    import torch
+
+    for n in args.n:
+        side = max(4, int(round(args.synthetic ** (1.0 / (n - 1)))))
+        screen = [side] * (n - 1)
+        P = side ** (n - 1)
+        g = torch.Generator(device="cpu").manual_seed(args.seed + n)
+        mean = torch.rand(P, 3, generator=g).cuda()
+        var = (torch.rand(P, 3, generator=g) * 0.01).cuda()
+        normal = torch.nn.functional.normalize(torch.randn(P, n, generator=g), dim=1).cuda()
+        depth = (torch.rand(P, generator=g) * 5 + 5).cuda()
+        target = (mean + 0.05 * torch.randn(P, 3, generator=g).cuda()).clamp_min(0).contiguous()
+        den = denoise.Denoiser(n, seed=args.seed)
+        den.set_input(screen, mean, var, normal, depth)
+        den.train_step(target, args.lr)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            den.train_step(target, args.lr)
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / max(1, args.steps)
+        t0 = time.perf_counter()
+        den.apply()
+        torch.cuda.synchronize()
+        fwd = time.perf_counter() - t0
+        L = den.layout
+        flops = 2 * P * (L["features_padded"] * L["hidden"] + L["hidden"] * L["hidden"] + L["hidden"] * L["outputs_padded"])
+        print(json.dumps({"n": n, "pixels": P, "train_step_ms": dt * 1e3, "apply_ms": fwd * 1e3,
+                          "forward_gemm_tflops_per_s": flops / fwd / 1e12}), flush=True)
+
+
 def main(argv=None) -> None:
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--n", type=int, nargs="+", default=[3, 4, 5])
@@ -142,7 +176,12 @@ def main(argv=None) -> None:
     ap.add_argument("--eval", action="store_true")
     ap.add_argument("--target", type=float, default=1e-2)
     ap.add_argument("--load", action="store_true", help="evaluate saved weights instead of training")
+    ap.add_argument("--synthetic", type=int, default=0,
+                    help="train on seeded synthetic inputs of this many pixels (kernel throughput; no rendering)")
     args = ap.parse_args(argv)
+    if args.synthetic:
+        synthetic(args)
+        return
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     for n in args.n:
