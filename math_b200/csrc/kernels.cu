@@ -1393,6 +1393,26 @@ cudaError_t launch_srgb_slice(const double* accum, long long samples, long long 
         return cudaGetLastError();
 }
 
+// per-pixel sums (doubles) -> mean colour (floats), for the accumulator read-back
+__global__ void k_mean(long long n3, const double* __restrict__ sums, double inv, float* __restrict__ out)
+{
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
+        {
+                out[i] = (float)(sums[i] * inv);
+        }
+}
+
+cudaError_t launch_mean(long long n3, const double* sums, long long samples, float* out, cudaStream_t st)
+{
+        if (n3 <= 0)
+        {
+                return cudaSuccess;
+        }
+        const unsigned g = (unsigned)std::min<long long>((n3 + BLOCK - 1) / BLOCK, 148LL * 32);
+        k_mean<<<g, BLOCK, 0, st>>>(n3, sums, samples > 0 ? 1.0 / (double)samples : 0.0, out);
+        return cudaGetLastError();
+}
+
 #define NT_INSTANTIATE(N)                                                                                         \
         template struct Wavefront<N>;                                                                             \
         template cudaError_t launch_trace_closest<N>(const MeshDev<N>&, const float*, const float*, long long, int, \

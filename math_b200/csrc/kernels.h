@@ -80,6 +80,9 @@ template <int N>
 cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, float* depth, cudaStream_t st);
 cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, float* mean, float* var, cudaStream_t st);
 
+// Mean colour per pixel (floats) from the per-pixel sums.
+cudaError_t launch_mean(long long n3, const double* sums, long long samples, float* out, cudaStream_t st);
+
 // Viewer feed: width x height words 0x00RRGGBB (sRGB) of the slice whose first pixel is `base`.
 cudaError_t launch_srgb_slice(const double* accum, long long samples, long long base, int width, int height,
                               long long row_stride, uint32_t* out, cudaStream_t st);

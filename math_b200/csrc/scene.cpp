@@ -328,6 +328,7 @@ struct nt_scene
         bool pool_smooth = false;
         DevBuf counters;
         DevBuf moments;  // per-path sums of nt_render_moments
+        DevBuf mean_buf; // mean colours for nt_accum_read
         unsigned long long* host_counters = nullptr;
         long long samples_done = 0;
         std::vector<unsigned char> dev_scene;  // packed DevScene<N>
@@ -2458,16 +2459,19 @@ int nt_accum_read(nt_scene* scene, float* rgb_mean, int64_t* samples_per_pixel)
                 {
                         return;
                 }
-                std::vector<double> sums((size_t)npix * 3);
-                check_cuda(cudaMemcpyAsync(sums.data(), scene->accum.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost,
-                                           scene->stream),
+                // the mean is formed on the device (the same double product, rounded once), so half the
+                // bytes cross to the host, straight into the caller's array
+                const size_t bytes = (size_t)npix * 3 * sizeof(float);
+                if (scene->mean_buf.bytes < bytes)
+                {
+                        scene->mean_buf.alloc(bytes);
+                }
+                check_cuda(launch_mean(npix * 3, scene->accum.as<double>(), scene->samples_done, scene->mean_buf.as<float>(),
+                                       scene->stream),
+                           "mean");
+                check_cuda(cudaMemcpyAsync(rgb_mean, scene->mean_buf.p, bytes, cudaMemcpyDeviceToHost, scene->stream),
                            "read accumulator");
                 check_cuda(cudaStreamSynchronize(scene->stream), "sync");
-                double inv = scene->samples_done > 0 ? 1.0 / (double)scene->samples_done : 0.0;
-                for (size_t i = 0; i < sums.size(); ++i)
-                {
-                        rgb_mean[i] = (float)(sums[i] * inv);
-                }
         });
 }
 

@@ -361,9 +361,13 @@ class Scene:
     def clear(self) -> None:
         _check(self._lib.nt_accum_clear(self._h))
 
-    def image(self) -> tuple[np.ndarray, int]:
-        """Mean colour per pixel, shape (pixels, 3), x0 fastest; and samples per pixel."""
-        out = np.zeros((self.pixel_count, 3), np.float32)
+    def image(self, out=None) -> tuple[np.ndarray, int]:
+        """Mean colour per pixel, shape (pixels, 3), x0 fastest; and samples per pixel.  out: an
+        optional float32 array of that shape to fill (e.g. a pinned buffer reused every frame)."""
+        if out is None:
+            out = np.zeros((self.pixel_count, 3), np.float32)
+        elif out.dtype != np.float32 or out.shape != (self.pixel_count, 3) or not out.flags.c_contiguous:
+            raise ValueError("out must be a contiguous float32 array of shape (pixels, 3)")
         spp = ctypes.c_int64()
         _check(self._lib.nt_accum_read(self._h, out.ctypes.data, ctypes.byref(spp)))
         return out, int(spp.value)
