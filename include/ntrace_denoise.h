@@ -5,10 +5,14 @@
  * render (nt_render) stays the fallback and the judge of the denoiser's error.  The network reads,
  * per pixel, the noisy mean radiance, the variance of that mean, the first-hit normal (n floats) and
  * depth, at the pixel and at its 2(n-1) neighbours along the screen axes, and predicts for each
- * screen axis 9 filter weights (softmax over taps -4..4); the filters are applied one axis after the
- * other to the noisy mean.  Layers: features -> 64 -> 64 -> 9(n-1), ReLU between, BF16 operands with
+ * screen axis a cross-bilateral filter of 9 taps (-4..4): 9 tap logits and 3 log-bandwidths o_g of
+ * the guides g (squared normal difference, squared depth difference, non-local-means colour distance
+ * between the pixel and the tap); tap weight = softmax over taps of logit - sum_g
+ * scale_g exp(min(o_g, 20)) D_g, scale = (64, 16, 1).  The filters are applied one axis after the
+ * other to the noisy mean.  Layers: features -> 64 -> 64 -> 12(n-1), ReLU between, BF16 operands with
  * FP32 accumulation on the tensor cores (tcgen05), FP32 master weights trained with Adam on the loss
- * sum((out - target)^2) / sum(target^2) (the square of the relative RMSE).
+ * sum((out - target)^2) / sum((noisy - target)^2): the squared error left relative to the input's, so
+ * that images of every noise level weigh alike in training.
  *
  * Inputs come from nt_render_moments and nt_render_aux (include/ntrace.h).  All image arrays are
  * device memory, pixels linear with x0 fastest, RGB as 3 floats per pixel.  Every function returns
@@ -33,7 +37,7 @@ typedef struct nt_denoiser_layout
         int features;         /* network inputs: base_features x (2(n-1) + 1) */
         int features_padded;  /* inputs rounded up to a multiple of 16 (the MMA K step) */
         int hidden;           /* 64 */
-        int outputs;          /* 9 (n-1) filter logits */
+        int outputs;          /* (9 + 3)(n-1): the 9 tap logits of every axis, then the 3 log-bandwidths of every axis */
         int outputs_padded;   /* rounded up to a multiple of 16 */
         int64_t param_count;  /* W1 (hidden x features), b1, W2 (hidden x hidden), b2, W3 (outputs x hidden), b3 */
 } nt_denoiser_layout;

@@ -33,6 +33,11 @@ constexpr int HID = 64;
 constexpr int TAPS = 9;
 constexpr int RADIUS = 4;
 constexpr int MAX_AXES = 5;
+// Guides of the cross-bilateral filter: normal, depth and colour distance between a pixel and a tap.
+// The network predicts, per screen axis, one log-bandwidth o per guide; the guide's weight on the
+// tap logits is GUIDE_SCALE x exp(min(o, BANDWIDTH_MAX)).
+constexpr int GUIDES = 3;
+constexpr float BANDWIDTH_MAX = 20.0f;
 
 // ------------------------------------------------------------------------------------------------
 // tcgen05 GEMM
@@ -522,28 +527,87 @@ __device__ __forceinline__ void softmax9(const float* z, float* w)
         }
 }
 
-// y_out[p] = sum_j softmax(Z[p, a*9 .. a*9+8])_j y_in[p + (j - 4) e_a]
-__global__ void k_filter_fwd(long long P, Stencil st, int a, const float* __restrict__ Z, int ldz,
-                             const float* __restrict__ y_in, float* __restrict__ y_out)
+__device__ __forceinline__ float guide_scale(int g)
+{
+        return g == 0 ? 64.0f : (g == 1 ? 16.0f : 1.0f);
+}
+
+// Guide distances between pixels p and q from the base features (mean 0..2, standard deviation of the
+// mean 3..5, normal 6..6+n-1, depth / 10 at 6+n): squared normal difference, squared depth
+// difference, and the colour distance of non-local-means filtering (Rousselle, Knaus and Zwicker,
+// "Adaptive rendering with non-local means filtering", 2012): the squared difference of the means
+// less the variance it carries from the noise, over that variance plus a small relative floor,
+// averaged over the channels.
+__device__ __forceinline__ void guide_distance(const float* __restrict__ base, int nf, long long p, long long q, float* D)
+{
+        const int n = nf - 7;
+        const float* bp = base + p * nf;
+        const float* bq = base + q * nf;
+        float dn = 0;
+        for (int k = 0; k < n; ++k)
+        {
+                const float t = bp[6 + k] - bq[6 + k];
+                dn += t * t;
+        }
+        const float dd = 10.0f * (bp[6 + n] - bq[6 + n]);
+        float dc = 0;
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+        {
+                const float dm = bp[c] - bq[c];
+                const float v = bp[3 + c] * bp[3 + c] + bq[3 + c] * bq[3 + c];
+                const float mb = 0.5f * (bp[c] + bq[c]);
+                dc += fmaxf(dm * dm - v, 0.0f) / (1e-4f + 0.01f * mb * mb + v);
+        }
+        D[0] = dn;
+        D[1] = dd * dd;
+        D[2] = dc * (1.0f / 3.0f);
+}
+
+// The axis's tap weights at pixel p: softmax over taps of Z[p, a*9 + j] - sum_g s_g D_g(p, tap j),
+// s_g = GUIDE_SCALE x exp(min(Z[p, 9 (n-1) + a*3 + g], BANDWIDTH_MAX)).  The taps' pixels q, D, s and
+// whether each log-bandwidth lies below its clamp are returned for the backward pass.
+__device__ __forceinline__ void tap_weights(const Stencil& st, const float* __restrict__ base, int a, long long p,
+                                            const float* __restrict__ Z, int ldz, long long* q, float (*D)[GUIDES],
+                                            float* s, bool* open, float* w)
+{
+        const float* zrow = Z + p * ldz;
+#pragma unroll
+        for (int g = 0; g < GUIDES; ++g)
+        {
+                const float o = zrow[st.axes * TAPS + a * GUIDES + g];
+                open[g] = o < BANDWIDTH_MAX;
+                s[g] = guide_scale(g) * expf(fminf(o, BANDWIDTH_MAX));
+        }
+        float z[TAPS];
+#pragma unroll
+        for (int j = 0; j < TAPS; ++j)
+        {
+                q[j] = st.neighbour(p, a, j - RADIUS);
+                guide_distance(base, st.nf, p, q[j], D[j]);
+                z[j] = zrow[a * TAPS + j] - (s[0] * D[j][0] + s[1] * D[j][1] + s[2] * D[j][2]);
+        }
+        softmax9(z, w);
+}
+
+// y_out[p] = sum_j w_j y_in[p + (j - 4) e_a] with the tap weights above
+__global__ void k_filter_fwd(long long P, Stencil st, int a, const float* __restrict__ base, const float* __restrict__ Z,
+                             int ldz, const float* __restrict__ y_in, float* __restrict__ y_out)
 {
         for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
         {
-                float z[TAPS], w[TAPS];
-#pragma unroll
-                for (int j = 0; j < TAPS; ++j)
-                {
-                        z[j] = Z[p * ldz + a * TAPS + j];
-                }
-                softmax9(z, w);
+                long long q[TAPS];
+                float D[TAPS][GUIDES], s[GUIDES], w[TAPS];
+                bool open[GUIDES];
+                tap_weights(st, base, a, p, Z, ldz, q, D, s, open, w);
                 float acc[3] = {0, 0, 0};
 #pragma unroll
                 for (int j = 0; j < TAPS; ++j)
                 {
-                        const long long q = st.neighbour(p, a, j - RADIUS);
 #pragma unroll
                         for (int c = 0; c < 3; ++c)
                         {
-                                acc[c] += w[j] * y_in[q * 3 + c];
+                                acc[c] += w[j] * y_in[q[j] * 3 + c];
                         }
                 }
 #pragma unroll
@@ -554,40 +618,50 @@ __global__ void k_filter_fwd(long long P, Stencil st, int a, const float* __rest
         }
 }
 
-// backward of k_filter_fwd: dZ for the axis's taps (through the softmax) and, when g_in is given,
-// dL/dy_in added by atomics
-__global__ void k_filter_bwd(long long P, Stencil st, int a, const float* __restrict__ Z, int ldz,
-                             const float* __restrict__ y_in, const float* __restrict__ g_out, float* g_in,
+// backward of k_filter_fwd: dZ for the axis's tap logits and log-bandwidths (through the softmax) and,
+// when g_in is given, dL/dy_in added by atomics
+__global__ void k_filter_bwd(long long P, Stencil st, int a, const float* __restrict__ base, const float* __restrict__ Z,
+                             int ldz, const float* __restrict__ y_in, const float* __restrict__ g_out, float* g_in,
                              __nv_bfloat16* __restrict__ dZ)
 {
         for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
         {
-                float z[TAPS], w[TAPS], dw[TAPS];
-#pragma unroll
-                for (int j = 0; j < TAPS; ++j)
-                {
-                        z[j] = Z[p * ldz + a * TAPS + j];
-                }
-                softmax9(z, w);
+                long long q[TAPS];
+                float D[TAPS][GUIDES], s[GUIDES], w[TAPS], dw[TAPS];
+                bool open[GUIDES];
+                tap_weights(st, base, a, p, Z, ldz, q, D, s, open, w);
                 const float g0 = g_out[p * 3], g1 = g_out[p * 3 + 1], g2 = g_out[p * 3 + 2];
                 float dot = 0;
 #pragma unroll
                 for (int j = 0; j < TAPS; ++j)
                 {
-                        const long long q = st.neighbour(p, a, j - RADIUS);
-                        dw[j] = g0 * y_in[q * 3] + g1 * y_in[q * 3 + 1] + g2 * y_in[q * 3 + 2];
+                        const long long qj = q[j];
+                        dw[j] = g0 * y_in[qj * 3] + g1 * y_in[qj * 3 + 1] + g2 * y_in[qj * 3 + 2];
                         dot += w[j] * dw[j];
                         if (g_in)
                         {
-                                atomicAdd(g_in + q * 3, w[j] * g0);
-                                atomicAdd(g_in + q * 3 + 1, w[j] * g1);
-                                atomicAdd(g_in + q * 3 + 2, w[j] * g2);
+                                atomicAdd(g_in + qj * 3, w[j] * g0);
+                                atomicAdd(g_in + qj * 3 + 1, w[j] * g1);
+                                atomicAdd(g_in + qj * 3 + 2, w[j] * g2);
                         }
                 }
+                float ds[GUIDES] = {0, 0, 0};
 #pragma unroll
                 for (int j = 0; j < TAPS; ++j)
                 {
-                        dZ[p * ldz + a * TAPS + j] = __float2bfloat16_rn(w[j] * (dw[j] - dot));
+                        const float gl = w[j] * (dw[j] - dot);
+                        dZ[p * ldz + a * TAPS + j] = __float2bfloat16_rn(gl);
+#pragma unroll
+                        for (int g = 0; g < GUIDES; ++g)
+                        {
+                                ds[g] -= gl * D[j][g];
+                        }
+                }
+                // d logit_j / d o_g = -s_g D_g(j), zero where the log-bandwidth is clamped
+#pragma unroll
+                for (int g = 0; g < GUIDES; ++g)
+                {
+                        dZ[p * ldz + st.axes * TAPS + a * GUIDES + g] = __float2bfloat16_rn(open[g] ? ds[g] * s[g] : 0.0f);
                 }
         }
 }
@@ -616,14 +690,14 @@ __device__ __forceinline__ double block_sum(double v, double* s_red)
         return t;
 }
 
-// sums[0] += sum(target^2)
-__global__ void k_energy(long long n3, const float* __restrict__ target, double* sums)
+// sums[0] += sum((noisy - target)^2), the squared error of the input
+__global__ void k_energy(long long n3, const float* __restrict__ noisy, const float* __restrict__ target, double* sums)
 {
         __shared__ double s_red[TB / 32];
         double acc = 0;
         for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n3; i += (long long)gridDim.x * blockDim.x)
         {
-                const double t = target[i];
+                const double t = (double)noisy[i] - (double)target[i];
                 acc += t * t;
         }
         const double b = block_sum(acc, s_red);
@@ -930,7 +1004,7 @@ void forward(nt_denoiser* d)
            "gemm 3");
         for (int a = 0; a < d->n - 1; ++a)
         {
-                k_filter_fwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->Z.as<float>(), d->Op,
+                k_filter_fwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->base.as<float>(), d->Z.as<float>(), d->Op,
                                                             d->Y.as<float>() + (size_t)a * P * 3,
                                                             d->Y.as<float>() + (size_t)(a + 1) * P * 3);
         }
@@ -946,7 +1020,7 @@ double backward(nt_denoiser* d, const float* target)
         int* err = d->err.as<int>();
         const int A = d->n - 1;
         ck(cudaMemsetAsync(d->sums.p, 0, 2 * sizeof(double), s), "memset");
-        k_energy<<<blocks_for(P * 3), TB, 0, s>>>(P * 3, target, d->sums.as<double>());
+        k_energy<<<blocks_for(P * 3), TB, 0, s>>>(P * 3, d->Y.as<float>(), target, d->sums.as<double>());
         float* G0 = d->G.as<float>();
         float* G1 = G0 + (size_t)P * 3;
         k_loss_grad<<<blocks_for(P * 3), TB, 0, s>>>(P * 3, d->Y.as<float>() + (size_t)A * P * 3, target,
@@ -960,7 +1034,7 @@ double backward(nt_denoiser* d, const float* target)
                 {
                         ck(cudaMemsetAsync(gin, 0, (size_t)P * 3 * sizeof(float), s), "memset");
                 }
-                k_filter_bwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->Z.as<float>(), d->Op,
+                k_filter_bwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->base.as<float>(), d->Z.as<float>(), d->Op,
                                                             d->Y.as<float>() + (size_t)a * P * 3, gout, a > 0 ? gin : nullptr,
                                                             d->dZ.as<__nv_bfloat16>());
                 std::swap(gout, gin);
@@ -1013,7 +1087,7 @@ int nt_denoiser_create(int n, uint64_t seed, nt_denoiser** out)
                 d->nf = n + 7;
                 d->F = d->nf * (2 * (n - 1) + 1);
                 d->Fp = (d->F + 15) / 16 * 16;
-                d->O = TAPS * (n - 1);
+                d->O = (TAPS + GUIDES) * (n - 1);
                 d->Op = (d->O + 15) / 16 * 16;
                 d->nparams = (long long)HID * d->F + HID + HID * HID + HID + (long long)d->O * HID + d->O;
                 ck(cudaStreamCreateWithFlags(&d->own, cudaStreamNonBlocking), "cudaStreamCreate");

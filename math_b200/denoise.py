@@ -19,6 +19,7 @@ from . import ntrace
 from .ntrace import NtraceError, _check
 
 TAPS = 9
+GUIDES = 3  # cross-bilateral guides per screen axis: normal, depth, colour
 
 
 class Layout(ctypes.Structure):
@@ -327,8 +328,12 @@ def evaluate(den: Denoiser, pairs: list[dict]) -> dict:
 
 
 def uniform_filter_params(den: Denoiser) -> np.ndarray:
-    """Parameters that make every filter tap weight 1/9 (the method without learning)."""
-    return np.zeros(den.param_count, np.float32)
+    """Parameters that make every filter tap weight 1/9 (the method without learning): tap logits 0
+    and every guide's log-bandwidth -40 (its weight on the logits below 1e-15)."""
+    p = np.zeros(den.param_count, np.float32)
+    A = den.n - 1
+    p[den.param_count - A * GUIDES:] = -40.0  # the last A x GUIDES biases of the output layer
+    return p
 
 
 def time_call(fn, repeat: int = 1) -> float:

@@ -6,14 +6,16 @@ measures the time to a relative RMSE of 1e-2 against a 64k-sample render, plain 
 Training pairs: seeded variations (light position, view direction, albedos in [0.3, 0.9]) of the
 measured scenes' meshes on small screens; the noisy input is a few samples per pixel (its per-pixel
 mean and variance of the mean), plus the first-hit normal and depth; the target is a 4096-sample
-render.  The input sample count of each pair is drawn from --spp-in, so one
-network covers several noise levels.  Weights go to <out>/denoiser_n<n>.npz.
+render.  The input sample count of each pair is k^(n-1) (a full stratification grid, k per screen
+axis) with k drawn from --k-in, so one network covers several noise levels.  Weights go to
+<out>/denoiser_n<n>.npz.
 
 Evaluation (--eval): a held-out variation at the measured configuration's screen size (400^2, 128^3,
-48^4); plain renders at 1, 4, 16, ... samples and denoised renders at each --spp-in, timed over the
-whole frame, give (time, relative RMSE) points, the error measured on the centred window (128^2,
-32^3, 16^4) against a 64k-sample render of that window (effective k^(n-1) >= 65536); the report is
-the time each method needs to reach --target.
+48^4); plain and denoised renders on the same sample grid, k^(n-1) samples for k = 1, 2, 3, ...,
+timed over the whole frame, give (time, relative RMSE) points, the error measured on the centred
+window (128^2, 32^3, 16^4) against a 64k-sample render of that window (effective k^(n-1) >= 65536);
+the report is the time each method needs to reach --target (its first grid point at or below it),
+and the plain time fitted to the target exactly (Monte Carlo error ~ 1/sqrt(spp), time ~ spp).
 """
 
 from __future__ import annotations
@@ -53,11 +55,11 @@ def mesh_for(n: int, small: bool = False):
     return scenes.make_spec(6, v, f, screen=TRAIN_SCREEN[6], spp=4)
 
 
-def make_mixed_pairs(scene, n: int, count: int, seed: int, spp_in: list[int], spp_ref: int) -> list[dict]:
+def make_mixed_pairs(scene, n: int, count: int, seed: int, k_in: list[int], spp_ref: int) -> list[dict]:
     pairs = []
     rng = np.random.default_rng(seed)
     for i in range(count):
-        s = int(spp_in[rng.integers(len(spp_in))])
+        s = int(k_in[rng.integers(len(k_in))]) ** (n - 1)
         pairs += denoise.make_pairs(scene, 1, seed=seed * 7919 + i, screen=TRAIN_SCREEN[n], spp_in=s, spp_ref=spp_ref,
                                     units_per_pixel=EXTENT / EVAL_SCREEN[n], extent=CROP_EXTENT)
     return pairs
@@ -70,10 +72,11 @@ def crop(img, n: int, full: int, size: int):
     return a[tuple([slice(o, o + size)] * (n - 1))].reshape(-1, 3)
 
 
-def time_to_rmse(scene, den, n: int, spp_in: list[int], target: float, seed: int, max_plain_spp: int = 1 << 12) -> dict:
+def time_to_rmse(scene, den, n: int, target: float, seed: int, max_plain_spp: int = 1 << 12) -> dict:
     """Plain and denoised renders of one held-out variation at the measured screen size, timed over
-    the whole frame; their error is measured on the centred window against a 64k-sample render of
-    that window (same pixel grid)."""
+    the whole frame, at k^(n-1) samples for k = 1, 2, ... until each reaches the target; their error
+    is measured on the centred window against a 64k-sample render of that window (same pixel
+    grid)."""
     import torch
 
     full, size = EVAL_SCREEN[n], REF_CROP[n]
@@ -86,9 +89,14 @@ def time_to_rmse(scene, den, n: int, spp_in: list[int], target: float, seed: int
     ref_s = time.perf_counter() - t0
     denoise.apply_variant(scene, v)
     plain = []
-    spp = 1
-    while spp <= max_plain_spp:
+    k = 1
+    while k ** (n - 1) <= max_plain_spp:
+        spp = k ** (n - 1)
+        # warm (graphs and pools of this sample count), then timed
         scene.clear()
+        scene.render(spp, max_depth=5, seed=seed + 3 + spp)
+        scene.clear()
+        torch.cuda.synchronize()
         t0 = time.perf_counter()
         scene.render(spp, max_depth=5, seed=seed + 2 + spp)
         dt = time.perf_counter() - t0
@@ -97,9 +105,12 @@ def time_to_rmse(scene, den, n: int, spp_in: list[int], target: float, seed: int
                       "rmse": denoise.relative_rmse(crop(img, n, full, size), ref)})
         if plain[-1]["rmse"] <= target:
             break
-        spp *= 4
+        k += 1
     den_pts = []
-    for s in spp_in:
+    k = 1
+    while k ** (n - 1) <= max_plain_spp:
+        s = k ** (n - 1)
+        k += 1
         # warm (the denoiser's workspace is allocated on first use)
         x = denoise.render_inputs(scene, s, seed=seed + 5)
         den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
@@ -107,25 +118,35 @@ def time_to_rmse(scene, den, n: int, spp_in: list[int], target: float, seed: int
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         x = denoise.render_inputs(scene, s, seed=seed + 7)
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
         den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
         out = den.apply()
         torch.cuda.synchronize()
-        dt = time.perf_counter() - t0
-        den_pts.append({"spp": ntrace.effective_spp(n, s), "seconds": dt,
-                        "rmse": denoise.relative_rmse(crop(out, n, full, size), ref),
+        t2 = time.perf_counter()
+        den_pts.append({"spp": ntrace.effective_spp(n, s), "seconds": t2 - t0, "render_seconds": t1 - t0,
+                        "network_seconds": t2 - t1, "rmse": denoise.relative_rmse(crop(out, n, full, size), ref),
                         "input_rmse": denoise.relative_rmse(crop(x["mean"], n, full, size), ref)})
+        if den_pts[-1]["rmse"] <= target:
+            break
 
     def first(points):
         ok = [p for p in points if p["rmse"] <= target]
         return min(ok, key=lambda p: p["seconds"]) if ok else None
 
     bp, bd = first(plain), first(den_pts)
+    # plain Monte Carlo error falls as 1/sqrt(spp) and its time grows as spp: the plain time at exactly
+    # the target, from its last grid point (the interpolation favours the plain render)
+    last = plain[-1]
+    plain_fit = last["seconds"] * (last["rmse"] / target) ** 2
     return {"n": n, "screen": [full] * (n - 1), "reference_window": [size] * (n - 1),
             "reference_spp": ntrace.effective_spp(n, REF_SPP), "reference_seconds": ref_s, "target_rmse": target,
             "plain": plain, "denoised": den_pts,
             "plain_time_to_target": bp["seconds"] if bp else None,
             "denoised_time_to_target": bd["seconds"] if bd else None,
-            "speedup": (bp["seconds"] / bd["seconds"]) if (bp and bd) else None}
+            "speedup": (bp["seconds"] / bd["seconds"]) if (bp and bd) else None,
+            "plain_time_to_target_fitted": plain_fit,
+            "speedup_vs_fitted": (plain_fit / bd["seconds"]) if bd else None}
 
 
 def synthetic(args) -> None:
@@ -168,7 +189,9 @@ def main(argv=None) -> None:
     ap.add_argument("--pairs", type=int, default=200)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--lr", type=float, default=1e-3)
-    ap.add_argument("--spp-in", type=int, nargs="+", default=[4, 16, 64])
+    ap.add_argument("--k-in", type=int, nargs="+", default=[1, 2, 3, 4, 6, 8],
+                    help="input samples per pixel of the training pairs: k^(n-1) for k drawn from these "
+                         "(those with k^(n-1) above spp-ref / 16 are left out)")
     ap.add_argument("--spp-ref", type=int, default=4096)
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--out", default=str(Path(__file__).resolve().parent / "weights"))
@@ -185,19 +208,20 @@ def main(argv=None) -> None:
     out = Path(args.out)
     out.mkdir(parents=True, exist_ok=True)
     for n in args.n:
+        k_in = [k for k in args.k_in if 16 * k ** (n - 1) <= args.spp_ref] or [1]
         t0 = time.perf_counter()
         spec = mesh_for(n, args.small)
         scene = scenes.build_scene(spec, tree_on_gpu=True)
         build_s = time.perf_counter() - t0
         path = out / f"denoiser_n{n}.npz"
-        report = {"n": n, "scene_build_seconds": build_s}
+        report = {"n": n, "scene_build_seconds": build_s, "k_in": k_in}
         if args.load:
             den = denoise.Denoiser.load(path)
         else:
             t0 = time.perf_counter()
-            pairs = make_mixed_pairs(scene, n, args.pairs, args.seed + n, args.spp_in, args.spp_ref)
+            pairs = make_mixed_pairs(scene, n, args.pairs, args.seed + n, k_in, args.spp_ref)
             report["pairs_seconds"] = time.perf_counter() - t0
-            held = make_mixed_pairs(scene, n, max(4, args.pairs // 10), args.seed + 1000 + n, args.spp_in,
+            held = make_mixed_pairs(scene, n, max(4, args.pairs // 10), args.seed + 1000 + n, k_in,
                                     args.spp_ref)
             den = denoise.Denoiser(n, seed=args.seed)
             uni = denoise.Denoiser(n, seed=args.seed)
@@ -211,7 +235,7 @@ def main(argv=None) -> None:
             den.save(path)
             report["weights"] = str(path)
         if args.eval:
-            report["time_to_rmse"] = time_to_rmse(scene, den, n, args.spp_in, args.target, seed=args.seed + 77 + n)
+            report["time_to_rmse"] = time_to_rmse(scene, den, n, args.target, seed=args.seed + 77 + n)
         print(json.dumps(report), flush=True)
         scene.close()
 

@@ -15,6 +15,11 @@ import numpy as np
 HID = 64
 TAPS = 9
 RADIUS = 4
+# cross-bilateral guides (normal, depth, colour): per screen axis the network predicts one
+# log-bandwidth o per guide, weighted GUIDE_SCALE x exp(min(o, BANDWIDTH_MAX)) on the tap logits
+GUIDES = 3
+GUIDE_SCALE = np.array([64.0, 16.0, 1.0])
+BANDWIDTH_MAX = 20.0
 
 
 def bf16(x: np.ndarray) -> np.ndarray:
@@ -28,7 +33,7 @@ def bf16(x: np.ndarray) -> np.ndarray:
 def layout(n: int) -> dict:
     nf = n + 7
     F = nf * (2 * (n - 1) + 1)
-    O = TAPS * (n - 1)
+    O = (TAPS + GUIDES) * (n - 1)
     return {"n": n, "base_features": nf, "features": F, "outputs": O, "hidden": HID,
             "param_count": HID * F + HID + HID * HID + HID + O * HID + O}
 
@@ -59,15 +64,37 @@ def neighbour_index(screen, a: int, d: int) -> np.ndarray:
     return idx + (y - x) * stride
 
 
-def features(n: int, screen, mean, var, normal, depth) -> np.ndarray:
-    """Network input per pixel: base features (mean, std of the mean, normal, depth / 10) at the pixel
-    and at its -1 / +1 neighbours along each screen axis, in that order."""
+def base_features(n: int, mean, var, normal, depth) -> np.ndarray:
+    """Per-pixel base features (float32): mean (3), standard deviation of the mean (3), normal (n),
+    depth / 10."""
     mean = np.asarray(mean, np.float32).reshape(-1, 3)
     var = np.asarray(var, np.float32).reshape(-1, 3)
     normal = np.asarray(normal, np.float32).reshape(-1, n)
     depth = np.asarray(depth, np.float32).reshape(-1)
-    base = np.concatenate([mean, np.sqrt(np.maximum(var, 0)).astype(np.float32), normal,
+    return np.concatenate([mean, np.sqrt(np.maximum(var, 0)).astype(np.float32), normal,
                            (depth * np.float32(0.1))[:, None]], axis=1)
+
+
+def guide_distances(base: np.ndarray, n: int, q: np.ndarray) -> np.ndarray:
+    """(P, 3) guide distances between every pixel and pixel q of it: squared normal difference,
+    squared depth difference, and the non-local-means colour distance (Rousselle, Knaus and Zwicker
+    2012): squared mean difference less its noise variance, clamped at 0, over that variance plus
+    1e-4 + 0.01 x (average mean)^2, averaged over the channels."""
+    bp = np.asarray(base, np.float64)
+    bq = bp[q]
+    dn = ((bp[:, 6:6 + n] - bq[:, 6:6 + n]) ** 2).sum(axis=1)
+    dd = (10.0 * (bp[:, 6 + n] - bq[:, 6 + n])) ** 2
+    dm = bp[:, :3] - bq[:, :3]
+    v = bp[:, 3:6] ** 2 + bq[:, 3:6] ** 2
+    mb = 0.5 * (bp[:, :3] + bq[:, :3])
+    dc = (np.maximum(dm ** 2 - v, 0) / (1e-4 + 0.01 * mb ** 2 + v)).sum(axis=1) / 3.0
+    return np.stack([dn, dd, dc], axis=1)
+
+
+def features(n: int, screen, mean, var, normal, depth) -> np.ndarray:
+    """Network input per pixel: base features (mean, std of the mean, normal, depth / 10) at the pixel
+    and at its -1 / +1 neighbours along each screen axis, in that order."""
+    base = base_features(n, mean, var, normal, depth)
     cols = [base]
     for a in range(n - 1):
         cols.append(base[neighbour_index(screen, a, -1)])
@@ -95,30 +122,42 @@ def forward(params: np.ndarray, n: int, screen, mean, var, normal, depth, bf16_p
     H2 = np.maximum(H1 @ W2.T + p["b2"], 0)
     H2 = r(H2.astype(np.float32)).astype(np.float64) if bf16_points else H2
     Z = H2 @ W3.T + p["b3"]
+    base = base_features(n, mean, var, normal, depth)
+    A = n - 1
     ys = [np.asarray(mean, np.float64).reshape(-1, 3)]
-    ws = []
-    for a in range(n - 1):
-        w = _softmax(Z[:, a * TAPS:(a + 1) * TAPS])
+    ws, Ds, ss = [], [], []
+    for a in range(A):
+        o = Z[:, A * TAPS + a * GUIDES:A * TAPS + (a + 1) * GUIDES]
+        s = GUIDE_SCALE * np.exp(np.minimum(o, BANDWIDTH_MAX))
+        logits = Z[:, a * TAPS:(a + 1) * TAPS].copy()
+        D = np.stack([guide_distances(base, n, neighbour_index(screen, a, j - RADIUS)) for j in range(TAPS)], axis=1)
+        logits -= (D * s[:, None, :]).sum(axis=2)
+        w = _softmax(logits)
         ws.append(w)
+        Ds.append(D)
+        ss.append(s * (o < BANDWIDTH_MAX))
         y = np.zeros_like(ys[-1])
         for j in range(TAPS):
             y += w[:, j:j + 1] * ys[-1][neighbour_index(screen, a, j - RADIUS)]
         ys.append(y)
-    return {"X": X, "W1": W1, "W2": W2, "W3": W3, "H1": H1, "H2": H2, "Z": Z, "ys": ys, "ws": ws, "out": ys[-1]}
+    return {"X": X, "W1": W1, "W2": W2, "W3": W3, "H1": H1, "H2": H2, "Z": Z, "ys": ys, "ws": ws, "Ds": Ds,
+            "ss": ss, "out": ys[-1]}
 
 
 def loss_and_grad(params: np.ndarray, n: int, screen, mean, var, normal, depth, target,
                   bf16_points: bool = True) -> tuple[float, np.ndarray]:
-    """Loss sum((out - target)^2) / sum(target^2) and its gradient (flat, parameter order)."""
+    """Loss sum((out - target)^2) / sum((noisy mean - target)^2) and its gradient (flat, parameter
+    order)."""
     f = forward(params, n, screen, mean, var, normal, depth, bf16_points)
     r = (lambda x: bf16(np.asarray(x, np.float32)).astype(np.float64)) if bf16_points else (lambda x: x)
     t = np.asarray(target, np.float64).reshape(-1, 3)
-    S = (t ** 2).sum()
+    S = ((f["ys"][0] - t) ** 2).sum()
     diff = f["out"] - t
     loss = float((diff ** 2).sum() / S)
     G = 2 * diff / S
     P = t.shape[0]
-    dZ = np.zeros((P, TAPS * (n - 1)))
+    A = n - 1
+    dZ = np.zeros((P, (TAPS + GUIDES) * A))
     for a in range(n - 2, -1, -1):
         w = f["ws"][a]
         y_in = f["ys"][a]
@@ -128,7 +167,10 @@ def loss_and_grad(params: np.ndarray, n: int, screen, mean, var, normal, depth, 
             q = neighbour_index(screen, a, j - RADIUS)
             dw[:, j] = (G * y_in[q]).sum(axis=1)
             np.add.at(G_in, q, w[:, j:j + 1] * G)
-        dZ[:, a * TAPS:(a + 1) * TAPS] = w * (dw - (w * dw).sum(axis=1, keepdims=True))
+        gl = w * (dw - (w * dw).sum(axis=1, keepdims=True))
+        dZ[:, a * TAPS:(a + 1) * TAPS] = gl
+        # d logit_j / d o_g = -s_g D_g(j) (0 where the log-bandwidth is clamped)
+        dZ[:, A * TAPS + a * GUIDES:A * TAPS + (a + 1) * GUIDES] = -(gl[:, :, None] * f["Ds"][a]).sum(axis=1) * f["ss"][a]
         G = G_in
     dZ = r(dZ)
     dH2 = r((dZ @ f["W3"]) * (f["H2"] > 0))

@@ -5,7 +5,7 @@ its bfloat16 rounding is round-to-nearest-even.  GPU: the tcgen05 GEMM against a
 product of the same bfloat16 operands; the network's output, loss and every parameter gradient
 against the oracle with the same rounding points; the moments and first-hit inputs against plain
 renders; and training on tracer-rendered pairs against the method without learning (every filter
-tap 1/9) on held-out pairs."""
+tap 1/9, guides off) on held-out pairs."""
 
 import numpy as np
 import pytest
@@ -19,7 +19,7 @@ def _random_inputs(n, screen, rng):
     var = rng.uniform(0.0, 0.05, (P, 3)).astype(np.float32)
     normal = rng.normal(size=(P, n)).astype(np.float32)
     normal /= np.linalg.norm(normal, axis=1, keepdims=True)
-    depth = rng.uniform(5.0, 12.0, P).astype(np.float32)
+    depth = rng.uniform(7.5, 8.5, P).astype(np.float32)
     target = np.clip(mean + rng.normal(0, 0.1, (P, 3)), 0, None).astype(np.float32)
     return mean, var, normal, depth, target
 
@@ -32,6 +32,21 @@ def _random_params(n, rng, scale=0.3):
     parts["W2"] *= 1.0 / np.sqrt(dor.HID)
     parts["b1"] = np.abs(parts["b1"]) * 0.1
     parts["b2"] = np.abs(parts["b2"]) * 0.1
+    # guide bandwidths of a few units: every guide changes the tap weights without saturating them
+    parts["b3"][_bandwidth_columns(n)] += np.tile([-3.5, -2.5, 0.0], n - 1)
+    return dor.join(parts)
+
+
+def _bandwidth_columns(n):
+    A = n - 1
+    return np.arange(A * dor.TAPS, A * (dor.TAPS + dor.GUIDES))
+
+
+def _box_params(n):
+    """Tap logits 0 and guide bandwidths exp(-40) x scale: the separable 9-tap box filter."""
+    L = dor.layout(n)
+    parts = dor.split(np.zeros(L["param_count"]), n)
+    parts["b3"][_bandwidth_columns(n)] = -40.0
     return dor.join(parts)
 
 
@@ -54,7 +69,10 @@ def test_oracle_backward_matches_finite_differences(n, screen):
     L = dor.layout(n)
     idx = rng.choice(L["param_count"], 48, replace=False)
     # include the biases and the last layer
-    idx = np.concatenate([idx, [L["param_count"] - 1, L["param_count"] - 10, dor.HID * L["features"] + 3]])
+    A = n - 1
+    bw = L["param_count"] - A * dor.GUIDES  # the first log-bandwidth bias (normal guide of axis 0)
+    idx = np.concatenate([idx, [L["param_count"] - 1, L["param_count"] - 10, dor.HID * L["features"] + 3,
+                                bw, bw + 1, bw + 2, bw - 1]])
     eps = 1e-6
     for i in idx:
         p1 = params.copy()
@@ -71,7 +89,7 @@ def test_oracle_uniform_filter_is_a_box_blur():
     n, screen = 3, (7, 6)
     rng = np.random.default_rng(3)
     mean, var, normal, depth, _ = _random_inputs(n, screen, rng)
-    params = np.zeros(dor.layout(n)["param_count"])
+    params = _box_params(n)
     out = dor.forward(params, n, screen, mean, var, normal, depth, bf16_points=False)["out"]
     # interior pixel: mean of the 9 x 9 neighbourhood (separable, clamped at the border)
     x0, x1 = 3, 3
@@ -80,6 +98,29 @@ def test_oracle_uniform_filter_is_a_box_blur():
     rows = np.clip(np.arange(x1 - 4, x1 + 5), 0, screen[1] - 1)
     expect = img[np.ix_(rows, cols)].reshape(-1, 3).mean(axis=0)
     np.testing.assert_allclose(out[x1 * screen[0] + x0], expect, rtol=1e-12)
+
+
+def test_oracle_normal_guide_keeps_edges():
+    """Two half-screens of different normal: with tap logits 0 and the normal guide at its base
+    bandwidth (64 per unit of squared normal difference), each half is averaged over itself only."""
+    n, screen = 3, (12, 5)
+    P = screen[0] * screen[1]
+    x0 = np.arange(P) % screen[0]
+    left = x0 < 6
+    rng = np.random.default_rng(8)
+    mean = np.where(left[:, None], 0.2, 0.7) + rng.uniform(-0.05, 0.05, (P, 3))
+    var = np.full((P, 3), 1e-2, np.float32)
+    normal = np.where(left[:, None], [0.0, 0.0, 1.0], [0.6, 0.0, 0.8]).astype(np.float32)
+    depth = np.full(P, 8.0, np.float32)
+    params = _box_params(n)
+    parts = dor.split(params.copy(), n)
+    parts["b3"][_bandwidth_columns(n)[0::dor.GUIDES]] = 0.0  # normal guide on, at 64
+    out = dor.forward(dor.join(parts), n, screen, mean, var, normal, depth, bf16_points=False)["out"]
+    box = dor.forward(params, n, screen, mean, var, normal, depth, bf16_points=False)["out"]
+    # |n_l - n_r|^2 = 0.4: every tap across the edge is weighted exp(-25.6) against the same side
+    for side, level in ((left, 0.2), (~left, 0.7)):
+        assert np.abs(out[side] - level).max() < 0.05
+    assert np.abs(box[x0 == 5] - 0.2).max() > 0.1  # the box filter mixes the halves at the edge
 
 
 # ------------------------------------------------------------------------------------------------
