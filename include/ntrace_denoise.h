@@ -4,11 +4,13 @@
  * No counterpart in the reference (templeblock/math's painter only accumulates samples); the plain
  * render (nt_render) stays the fallback and the judge of the denoiser's error.  The network reads,
  * per pixel, the noisy mean radiance, the variance of that mean, the first-hit normal (n floats) and
- * depth, at the pixel and at its 2(n-1) neighbours along the screen axes, and predicts for each
+ * depth, and a spatial noise estimate (from the mean's differences to the axis neighbours, defined
+ * at one sample per pixel too), at the pixel and at its 2(n-1) neighbours along the screen axes,
+ * and the input's noise level 1/sqrt(samples per pixel), and predicts for each
  * screen axis a cross-bilateral filter of 9 taps (-4..4): 9 tap logits and 3 log-bandwidths o_g of
  * the guides g (squared normal difference, squared depth difference, non-local-means colour distance
  * between the pixel and the tap); tap weight = softmax over taps of logit - sum_g
- * scale_g exp(min(o_g, 20)) D_g, scale = (64, 16, 1).  The filters are applied one axis after the
+ * scale_g exp(min(o_g, 20)) D_g, scale = (4, 1, 0.05).  The filters are applied one axis after the
  * other to the noisy mean.  Layers: features -> 64 -> 64 -> 12(n-1), ReLU between, BF16 operands with
  * FP32 accumulation on the tensor cores (tcgen05), FP32 master weights trained with Adam on the loss
  * sum((out - target)^2) / sum((noisy - target)^2): the squared error left relative to the input's, so
@@ -33,8 +35,8 @@ typedef struct nt_denoiser nt_denoiser;
 typedef struct nt_denoiser_layout
 {
         int n;                /* space dimension (3..6); the screen has n-1 axes */
-        int base_features;    /* per-pixel features: 3 mean + 3 std + n normal + 1 depth = n + 7 */
-        int features;         /* network inputs: base_features x (2(n-1) + 1) */
+        int base_features;    /* per-pixel features: 3 mean + 3 std + n normal + 1 depth + 3 spatial noise = n + 10 */
+        int features;         /* network inputs: base_features x (2(n-1) + 1), then the noise level */
         int features_padded;  /* inputs rounded up to a multiple of 16 (the MMA K step) */
         int hidden;           /* 64 */
         int outputs;          /* (9 + 3)(n-1): the 9 tap logits of every axis, then the 3 log-bandwidths of every axis */
@@ -52,11 +54,12 @@ int nt_denoiser_get_layout(nt_denoiser* d, nt_denoiser_layout* out);
 int nt_denoiser_get_params(nt_denoiser* d, float* params);
 int nt_denoiser_set_params(nt_denoiser* d, const float* params);
 
-/* The noisy image to work on: screen (n-1 ints), per-pixel mean (x3), variance of the mean (x3),
- * first-hit normal (x n) and depth (x1), all device arrays.  stream: a cudaStream_t or NULL (the
+/* The noisy image to work on: screen (n-1 ints), the samples per pixel it was rendered with (the
+ * network reads 1/sqrt of it as the input's noise level), per-pixel mean (x3), variance of the mean
+ * (x3), first-hit normal (x n) and depth (x1), all device arrays.  stream: a cudaStream_t or NULL (the
  * denoiser's own stream); every later call on this input uses the same stream. */
-int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, const float* d_mean, const float* d_var,
-                          const float* d_normal, const float* d_depth, void* stream);
+int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, int samples_per_pixel, const float* d_mean,
+                          const float* d_var, const float* d_normal, const float* d_depth, void* stream);
 
 /* Denoised image of the current input into d_out (pixel_count x 3). */
 int nt_denoiser_apply(nt_denoiser* d, float* d_out);

@@ -167,7 +167,23 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
         bool pending = false;
         for (int kc = kb; kc < ke; kc += GK)
         {
-                if (LA::ROW_FAST)
+                if constexpr (LA::VEC8)
+                {
+                        // 16-byte chunks, eight consecutive rows fastest: a quarter warp's stores fill
+                        // one 128-byte block of core-matrix rows (no bank conflicts)
+                        for (int idx = tid; idx < GM * (GK / 8); idx += GTHREADS)
+                        {
+                                const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
+                                const int k8 = ((idx >> 3) % (GK / 8)) * 8;
+                                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                                if (m0 + r < M && kc + k8 < ke)
+                                {
+                                        v = la.load8(m0 + r, kc + k8);
+                                }
+                                *reinterpret_cast<uint4*>(sA + tile_off(r, k8)) = v;
+                        }
+                }
+                else if (LA::ROW_FAST)
                 {
                         for (int idx = tid; idx < GM * GK; idx += GTHREADS)
                         {
@@ -185,7 +201,21 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
                                 *reinterpret_cast<__nv_bfloat16*>(sA + tile_off(r, k)) = __float2bfloat16_rn(v);
                         }
                 }
-                if (LB::ROW_FAST)
+                if constexpr (LB::VEC8)
+                {
+                        for (int idx = tid; idx < N * (GK / 8); idx += GTHREADS)
+                        {
+                                const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
+                                const int k8 = ((idx >> 3) % (GK / 8)) * 8;
+                                uint4 v = make_uint4(0u, 0u, 0u, 0u);
+                                if (kc + k8 < ke)
+                                {
+                                        v = lb.load8(r, kc + k8);
+                                }
+                                *reinterpret_cast<uint4*>(sB + tile_off(r, k8)) = v;
+                        }
+                }
+                else if (LB::ROW_FAST)
                 {
                         for (int idx = tid; idx < N * GK; idx += GTHREADS)
                         {
@@ -273,20 +303,27 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
 
 // ---- operand loaders ----
 
-struct LoadRows  // A(r, k) = p[r * ld + k], BF16
+// A(r, k) = p[r * ld + k], BF16; VEC8: eight consecutive k (k a multiple of 8) as one 16-byte load,
+// which needs p 16-byte aligned and ld a multiple of 8
+struct LoadRows
 {
-        static constexpr bool ROW_FAST = false;
+        static constexpr bool VEC8 = true;
         const __nv_bfloat16* p;
         int ld;
-        __device__ __forceinline__ float operator()(int r, int k) const
+        __device__ __forceinline__ uint4 load8(int r, int k) const
         {
-                return __bfloat162float(p[(size_t)r * ld + k]);
+                return __ldg(reinterpret_cast<const uint4*>(p + (size_t)r * ld + k));
+        }
+        bool vec8_ok() const
+        {
+                return ((uintptr_t)p & 15u) == 0 && ld % 8 == 0;
         }
 };
 
 struct LoadCols  // A(r, k) = p[k * ld + r], BF16 (the transpose of a row-major matrix)
 {
         static constexpr bool ROW_FAST = true;
+        static constexpr bool VEC8 = false;
         const __nv_bfloat16* p;
         int ld;
         __device__ __forceinline__ float operator()(int r, int k) const
@@ -302,7 +339,9 @@ struct Stencil
         int size[MAX_AXES];
         long long stride[MAX_AXES];
         int nf;                     // base features per pixel
-        int features;               // nf x (2 axes + 1)
+        int stencil_features;       // nf x (2 axes + 1)
+        int features;               // stencil_features + 1: the noise level of the input last
+        float noise_level;          // 1 / sqrt(samples per pixel)
 
         // pixel at offset d along axis a from p, clamped to the screen
         __device__ __forceinline__ long long neighbour(long long p, int a, int d) const
@@ -314,9 +353,9 @@ struct Stencil
         // input feature k of pixel p
         __device__ __forceinline__ float feature(const float* base, long long p, int k) const
         {
-                if (k >= features)
+                if (k >= stencil_features)
                 {
-                        return 0.0f;
+                        return k == stencil_features ? noise_level : 0.0f;
                 }
                 const int q = k / nf;
                 const int f = k - q * nf;
@@ -330,27 +369,26 @@ struct Stencil
         }
 };
 
-struct LoadFeatures  // A(pixel, feature)
+// The network's input matrix X (pixels x padded features, BF16), written once per input: thread
+// (pixel, chunk) forms eight consecutive features and stores them as one 16-byte word, so that
+// consecutive threads write consecutive chunks of a row.
+__global__ void k_features(long long P, Stencil st, int Fp, const float* __restrict__ base, __nv_bfloat16* __restrict__ X)
 {
-        static constexpr bool ROW_FAST = false;
-        const float* base;
-        Stencil st;
-        __device__ __forceinline__ float operator()(int r, int k) const
+        const int chunks = Fp / 8;
+        const long long total = P * chunks;
+        for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
         {
-                return st.feature(base, r, k);
+                const long long p = i / chunks;
+                const int c = (int)(i - p * chunks);
+                __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                {
+                        v[j] = __float2bfloat16_rn(st.feature(base, p, c * 8 + j));
+                }
+                *reinterpret_cast<uint4*>(X + p * Fp + c * 8) = *reinterpret_cast<const uint4*>(v);
         }
-};
-
-struct LoadFeaturesT  // B(feature, pixel)
-{
-        static constexpr bool ROW_FAST = true;
-        const float* base;
-        Stencil st;
-        __device__ __forceinline__ float operator()(int r, int k) const
-        {
-                return st.feature(base, k, r);
-        }
-};
+}
 
 // ---- epilogues ----
 
@@ -368,6 +406,8 @@ struct EpiStoreF32
         }
 };
 
+// The epilogues below store a row's 16 columns as 16-byte words: out 16-byte aligned and ld a
+// multiple of 16 (every matrix they write has 64 or outputs_padded columns).
 struct EpiBiasF32
 {
         const float* bias;
@@ -375,10 +415,12 @@ struct EpiBiasF32
         int ld;
         __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
         {
+                float4* o = reinterpret_cast<float4*>(out + (size_t)row * ld + c0);
 #pragma unroll
-                for (int j = 0; j < 16; ++j)
+                for (int j = 0; j < 4; ++j)
                 {
-                        out[(size_t)row * ld + c0 + j] = v[j] + bias[c0 + j];
+                        o[j] = make_float4(v[4 * j] + bias[c0 + 4 * j], v[4 * j + 1] + bias[c0 + 4 * j + 1],
+                                           v[4 * j + 2] + bias[c0 + 4 * j + 2], v[4 * j + 3] + bias[c0 + 4 * j + 3]);
                 }
         }
 };
@@ -390,11 +432,15 @@ struct EpiBiasReluBF16
         int ld;
         __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
         {
+                __align__(16) __nv_bfloat16 h[16];
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
                 {
-                        out[(size_t)row * ld + c0 + j] = __float2bfloat16_rn(fmaxf(v[j] + bias[c0 + j], 0.0f));
+                        h[j] = __float2bfloat16_rn(fmaxf(v[j] + bias[c0 + j], 0.0f));
                 }
+                uint4* o = reinterpret_cast<uint4*>(out + (size_t)row * ld + c0);
+                o[0] = reinterpret_cast<const uint4*>(h)[0];
+                o[1] = reinterpret_cast<const uint4*>(h)[1];
         }
 };
 
@@ -406,12 +452,19 @@ struct EpiMaskBF16
         int ld;
         __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
         {
+                __align__(16) __nv_bfloat16 a[16];
+                __align__(16) __nv_bfloat16 h[16];
+                const uint4* pa = reinterpret_cast<const uint4*>(act + (size_t)row * ld + c0);
+                reinterpret_cast<uint4*>(a)[0] = pa[0];
+                reinterpret_cast<uint4*>(a)[1] = pa[1];
 #pragma unroll
                 for (int j = 0; j < 16; ++j)
                 {
-                        const size_t i = (size_t)row * ld + c0 + j;
-                        out[i] = __float2bfloat16_rn(__bfloat162float(act[i]) > 0.0f ? v[j] : 0.0f);
+                        h[j] = __float2bfloat16_rn(__bfloat162float(a[j]) > 0.0f ? v[j] : 0.0f);
                 }
+                uint4* o = reinterpret_cast<uint4*>(out + (size_t)row * ld + c0);
+                o[0] = reinterpret_cast<const uint4*>(h)[0];
+                o[1] = reinterpret_cast<const uint4*>(h)[1];
         }
 };
 
@@ -456,6 +509,21 @@ cudaError_t gemm(const LA& la, const LB& lb, const EPI& epi, int M, int N, int K
         {
                 return cudaErrorInvalidValue;
         }
+        // 16-byte operand chunks lie wholly inside or outside a CTA's K range when K is a multiple of 8
+        if constexpr (LA::VEC8)
+        {
+                if (!la.vec8_ok() || K % 8 != 0)
+                {
+                        return cudaErrorInvalidValue;
+                }
+        }
+        if constexpr (LB::VEC8)
+        {
+                if (!lb.vec8_ok() || K % 8 != 0)
+                {
+                        return cudaErrorInvalidValue;
+                }
+        }
         const uint32_t ncols = tmem_cols(N);
         // at most 512 / ncols CTAs share an SM's tensor memory: ask for enough shared memory that no
         // more are resident (an allocation then never waits)
@@ -483,17 +551,24 @@ unsigned blocks_for(long long n)
         return (unsigned)std::min<long long>((n + TB - 1) / TB, 148LL * 64);
 }
 
-// per-pixel base features: mean (3), standard deviation of the mean (3), normal (n), depth / 10
-__global__ void k_base_features(long long P, int n, const float* __restrict__ mean, const float* __restrict__ var,
+// per-pixel base features: mean (3), standard deviation of the mean (3), normal (n), depth / 10, and
+// the spatial noise estimate (3): sqrt of half the mean squared difference of the mean to the 2(n-1)
+// axis neighbours (clamped), which for independent noise over a locally constant image is the
+// standard deviation of the mean; unlike the per-pixel estimate it exists at one sample per pixel
+__global__ void k_base_features(long long P, Stencil st, const float* __restrict__ mean, const float* __restrict__ var,
                                 const float* __restrict__ normal, const float* __restrict__ depth, float* __restrict__ out)
 {
-        const int nf = n + 7;
+        const int nf = st.nf;
+        const int n = nf - 10;
+        const float inv = 1.0f / (float)(4 * st.axes);
         for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
         {
                 float* o = out + p * nf;
+                float m[3], sq[3] = {0, 0, 0};
                 for (int c = 0; c < 3; ++c)
                 {
-                        o[c] = mean[p * 3 + c];
+                        m[c] = mean[p * 3 + c];
+                        o[c] = m[c];
                         o[3 + c] = sqrtf(fmaxf(var[p * 3 + c], 0.0f));
                 }
                 for (int k = 0; k < n; ++k)
@@ -501,6 +576,22 @@ __global__ void k_base_features(long long P, int n, const float* __restrict__ me
                         o[6 + k] = normal[p * n + k];
                 }
                 o[6 + n] = depth[p] * 0.1f;
+                for (int a = 0; a < st.axes; ++a)
+                {
+                        for (int d = -1; d <= 1; d += 2)
+                        {
+                                const long long q = st.neighbour(p, a, d);
+                                for (int c = 0; c < 3; ++c)
+                                {
+                                        const float t = mean[q * 3 + c] - m[c];
+                                        sq[c] += t * t;
+                                }
+                        }
+                }
+                for (int c = 0; c < 3; ++c)
+                {
+                        o[7 + n + c] = sqrtf(sq[c] * inv);
+                }
         }
 }
 
@@ -527,20 +618,22 @@ __device__ __forceinline__ void softmax9(const float* z, float* w)
         }
 }
 
+// base bandwidths: at log-bandwidth 0 an object boundary (squared normal difference about 1) or a
+// depth step of a unit costs a tap a few units of logit, the colour term only a clear edge
 __device__ __forceinline__ float guide_scale(int g)
 {
-        return g == 0 ? 64.0f : (g == 1 ? 16.0f : 1.0f);
+        return g == 0 ? 4.0f : (g == 1 ? 1.0f : 0.05f);
 }
 
 // Guide distances between pixels p and q from the base features (mean 0..2, standard deviation of the
-// mean 3..5, normal 6..6+n-1, depth / 10 at 6+n): squared normal difference, squared depth
+// mean 3..5, normal 6..6+n-1, depth / 10 at 6+n, spatial noise 7+n..9+n): squared normal difference, squared depth
 // difference, and the colour distance of non-local-means filtering (Rousselle, Knaus and Zwicker,
 // "Adaptive rendering with non-local means filtering", 2012): the squared difference of the means
 // less the variance it carries from the noise, over that variance plus a small relative floor,
 // averaged over the channels.
 __device__ __forceinline__ void guide_distance(const float* __restrict__ base, int nf, long long p, long long q, float* D)
 {
-        const int n = nf - 7;
+        const int n = nf - 10;
         const float* bp = base + p * nf;
         const float* bq = base + q * nf;
         float dn = 0;
@@ -947,7 +1040,7 @@ struct nt_denoiser
         Buf gblock;
         float *gW1 = nullptr, *gb1 = nullptr, *gW2 = nullptr, *gb2 = nullptr, *gW3 = nullptr, *gb3 = nullptr;
         // per-image workspace
-        Buf base, H1, H2, Z, Y, G, dZ, dH1, dH2, sums, err;
+        Buf base, X, H1, H2, Z, Y, G, dZ, dH1, dH2, sums, err;
         bool packed = false;
 
         size_t gbytes() const
@@ -993,7 +1086,7 @@ void forward(nt_denoiser* d)
         const int P32 = (int)P;
         cudaStream_t s = d->st_use;
         int* err = d->err.as<int>();
-        ck(gemm(LoadFeatures{d->base.as<float>(), d->st}, LoadRows{d->W1.as<__nv_bfloat16>(), d->Fp},
+        ck(gemm(LoadRows{d->X.as<__nv_bfloat16>(), d->Fp}, LoadRows{d->W1.as<__nv_bfloat16>(), d->Fp},
                 EpiBiasReluBF16{d->b1.as<float>(), d->H1.as<__nv_bfloat16>(), HID}, P32, HID, d->Fp, 0, err, s),
            "gemm 1");
         ck(gemm(LoadRows{d->H1.as<__nv_bfloat16>(), HID}, LoadRows{d->W2.as<__nv_bfloat16>(), HID},
@@ -1056,7 +1149,7 @@ double backward(nt_denoiser* d, const float* target)
         ck(gemm(LoadCols{d->dH2.as<__nv_bfloat16>(), HID}, LoadCols{d->H1.as<__nv_bfloat16>(), HID},
                 EpiAtomicF32{d->gW2, HID, HID}, HID, HID, P32, kpc, err, s),
            "gemm dW2");
-        ck(gemm(LoadCols{d->dH1.as<__nv_bfloat16>(), HID}, LoadFeaturesT{d->base.as<float>(), d->st},
+        ck(gemm(LoadCols{d->dH1.as<__nv_bfloat16>(), HID}, LoadCols{d->X.as<__nv_bfloat16>(), d->Fp},
                 EpiAtomicF32{d->gW1, d->Fp, d->Fp}, HID, d->Fp, P32, kpc, err, s),
            "gemm dW1");
         const unsigned cb = (unsigned)std::min<long long>((P + 3) / 4, 1024);
@@ -1084,8 +1177,8 @@ int nt_denoiser_create(int n, uint64_t seed, nt_denoiser** out)
                 }
                 auto d = std::make_unique<nt_denoiser>();
                 d->n = n;
-                d->nf = n + 7;
-                d->F = d->nf * (2 * (n - 1) + 1);
+                d->nf = n + 10;
+                d->F = d->nf * (2 * (n - 1) + 1) + 1;
                 d->Fp = (d->F + 15) / 16 * 16;
                 d->O = (TAPS + GUIDES) * (n - 1);
                 d->Op = (d->O + 15) / 16 * 16;
@@ -1202,13 +1295,17 @@ int nt_denoiser_set_params(nt_denoiser* d, const float* params)
         });
 }
 
-int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, const float* d_mean, const float* d_var,
-                          const float* d_normal, const float* d_depth, void* stream)
+int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, int samples_per_pixel, const float* d_mean,
+                          const float* d_var, const float* d_normal, const float* d_depth, void* stream)
 {
         return guard([&]() {
                 if (!d || !screen || !d_mean || !d_var || !d_normal || !d_depth)
                 {
                         throw DError{NT_EINVAL, "null argument"};
+                }
+                if (samples_per_pixel < 1)
+                {
+                        throw DError{NT_EINVAL, "samples_per_pixel must be positive"};
                 }
                 Stencil st{};
                 st.axes = d->n - 1;
@@ -1228,11 +1325,14 @@ int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, const float* d_
                         throw DError{NT_EINVAL, "too many pixels for the denoiser"};
                 }
                 st.nf = d->nf;
+                st.stencil_features = d->F - 1;
                 st.features = d->F;
+                st.noise_level = (float)(1.0 / std::sqrt((double)samples_per_pixel));
                 d->st = st;
                 d->P = P;
                 d->st_use = stream ? (cudaStream_t)stream : d->own;
                 d->base.ensure(sizeof(float) * (size_t)P * d->nf);
+                d->X.ensure(sizeof(__nv_bfloat16) * (size_t)P * d->Fp);
                 d->H1.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
                 d->H2.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
                 d->dH1.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
@@ -1241,8 +1341,10 @@ int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, const float* d_
                 d->dZ.ensure(sizeof(__nv_bfloat16) * (size_t)P * d->Op);
                 d->Y.ensure(sizeof(float) * (size_t)P * 3 * d->n);
                 d->G.ensure(sizeof(float) * (size_t)P * 3 * 2);
-                k_base_features<<<blocks_for(P), TB, 0, d->st_use>>>(P, d->n, d_mean, d_var, d_normal, d_depth,
+                k_base_features<<<blocks_for(P), TB, 0, d->st_use>>>(P, st, d_mean, d_var, d_normal, d_depth,
                                                                       d->base.as<float>());
+                k_features<<<blocks_for(P * (d->Fp / 8)), TB, 0, d->st_use>>>(P, st, d->Fp, d->base.as<float>(),
+                                                                              d->X.as<__nv_bfloat16>());
                 ck(cudaGetLastError(), "features");
                 ck(cudaMemcpyAsync(d->Y.p, d_mean, sizeof(float) * (size_t)P * 3, cudaMemcpyDeviceToDevice, d->st_use),
                    "copy");

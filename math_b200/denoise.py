@@ -45,7 +45,7 @@ def _lib() -> ctypes.CDLL:
             "nt_denoiser_get_layout": ([vp, ctypes.POINTER(Layout)], ctypes.c_int),
             "nt_denoiser_get_params": ([vp, vp], ctypes.c_int),
             "nt_denoiser_set_params": ([vp, vp], ctypes.c_int),
-            "nt_denoiser_set_input": ([vp, vp, vp, vp, vp, vp, vp], ctypes.c_int),
+            "nt_denoiser_set_input": ([vp, vp, ctypes.c_int, vp, vp, vp, vp, vp], ctypes.c_int),
             "nt_denoiser_apply": ([vp, vp], ctypes.c_int),
             "nt_denoiser_gradient": ([vp, vp, vp, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "nt_denoiser_train_step": ([vp, vp, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
@@ -134,13 +134,14 @@ class Denoiser:
             k += size
         return out
 
-    def set_input(self, screen, mean, var, normal, depth, stream: int = 0) -> None:
+    def set_input(self, screen, mean, var, normal, depth, spp: int, stream: int = 0) -> None:
+        """The noisy image (device tensors) rendered with spp samples per pixel."""
         scr = np.ascontiguousarray(np.asarray(screen, np.int32))
         if scr.size != self.n - 1:
             raise ValueError("screen needs n - 1 sizes")
         self.pixels = int(np.prod(scr))
-        _check(self._lib.nt_denoiser_set_input(self._h, scr.ctypes.data, _dev(mean), _dev(var), _dev(normal), _dev(depth),
-                                               stream or None))
+        _check(self._lib.nt_denoiser_set_input(self._h, scr.ctypes.data, int(spp), _dev(mean), _dev(var), _dev(normal),
+                                               _dev(depth), stream or None))
         self._stream = stream
 
     def apply(self, out=None):
@@ -246,9 +247,10 @@ def apply_variant(scene: ntrace.Scene, v: dict, has_floor: bool = True) -> None:
     scene.build()
 
 
-def render_inputs(scene: ntrace.Scene, spp: int, seed: int, max_depth: int = 5, sample_offset: int = 0) -> dict:
+def render_inputs(scene: ntrace.Scene, spp: int, seed: int, max_depth: int = 5, sample_offset: int = 0,
+                  timing: dict | None = None) -> dict:
     """Noisy input of the denoiser: one pass of spp samples per pixel (per-pixel mean and variance of
-    the mean) plus the first-hit normal and depth."""
+    the mean) plus the first-hit normal and depth.  timing: filled with the seconds of each part."""
     import torch
 
     P, n = scene.pixel_count, scene.n
@@ -259,9 +261,15 @@ def render_inputs(scene: ntrace.Scene, spp: int, seed: int, max_depth: int = 5, 
         "depth": torch.empty((P,), dtype=torch.float32, device="cuda"),
     }
     torch.cuda.synchronize()
+    t0 = time.perf_counter()
     scene.render_moments(spp, out["mean"].data_ptr(), out["var"].data_ptr(), sample_offset=sample_offset,
                          max_depth=max_depth, seed=seed)
+    t1 = time.perf_counter()
     scene.render_aux(out["normal"].data_ptr(), out["depth"].data_ptr())
+    if timing is not None:
+        torch.cuda.synchronize()
+        timing["moments_seconds"] = t1 - t0
+        timing["aux_seconds"] = time.perf_counter() - t1
     return out
 
 
@@ -289,12 +297,13 @@ def make_pairs(scene: ntrace.Scene, count: int, seed: int, screen: int, spp_in: 
         x = render_inputs(scene, spp_in, seed=seed * 100003 + 2 * i, max_depth=max_depth)
         x["target"] = render_reference(scene, spp_ref, seed=seed * 100003 + 2 * i + 1, max_depth=max_depth)
         x["screen"] = list(v["screen"])
+        x["spp"] = ntrace.effective_spp(n, spp_in)
         pairs.append(x)
     return pairs
 
 
 def set_pair(den: Denoiser, pair: dict) -> None:
-    den.set_input(pair["screen"], pair["mean"], pair["var"], pair["normal"], pair["depth"])
+    den.set_input(pair["screen"], pair["mean"], pair["var"], pair["normal"], pair["depth"], pair["spp"])
 
 
 def train(den: Denoiser, pairs: list[dict], steps: int, lr: float = 1e-3, seed: int = 0, log=None) -> list[float]:

@@ -113,19 +113,21 @@ def time_to_rmse(scene, den, n: int, target: float, seed: int, max_plain_spp: in
         k += 1
         # warm (the denoiser's workspace is allocated on first use)
         x = denoise.render_inputs(scene, s, seed=seed + 5)
-        den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
+        den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"], s)
         den.apply()
         torch.cuda.synchronize()
+        parts = {}
         t0 = time.perf_counter()
-        x = denoise.render_inputs(scene, s, seed=seed + 7)
+        x = denoise.render_inputs(scene, s, seed=seed + 7, timing=parts)
         torch.cuda.synchronize()
         t1 = time.perf_counter()
-        den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"])
+        den.set_input(v["screen"], x["mean"], x["var"], x["normal"], x["depth"], s)
         out = den.apply()
         torch.cuda.synchronize()
         t2 = time.perf_counter()
         den_pts.append({"spp": ntrace.effective_spp(n, s), "seconds": t2 - t0, "render_seconds": t1 - t0,
-                        "network_seconds": t2 - t1, "rmse": denoise.relative_rmse(crop(out, n, full, size), ref),
+                        "network_seconds": t2 - t1, **parts,
+                        "rmse": denoise.relative_rmse(crop(out, n, full, size), ref),
                         "input_rmse": denoise.relative_rmse(crop(x["mean"], n, full, size), ref)})
         if den_pts[-1]["rmse"] <= target:
             break
@@ -165,7 +167,7 @@ def synthetic(args) -> None:
         depth = (torch.rand(P, generator=g) * 5 + 5).cuda()
         target = (mean + 0.05 * torch.randn(P, 3, generator=g).cuda()).clamp_min(0).contiguous()
         den = denoise.Denoiser(n, seed=args.seed)
-        den.set_input(screen, mean, var, normal, depth)
+        den.set_input(screen, mean, var, normal, depth, 4)
         den.train_step(target, args.lr)
         torch.cuda.synchronize()
         t0 = time.perf_counter()

@@ -18,7 +18,7 @@ RADIUS = 4
 # cross-bilateral guides (normal, depth, colour): per screen axis the network predicts one
 # log-bandwidth o per guide, weighted GUIDE_SCALE x exp(min(o, BANDWIDTH_MAX)) on the tap logits
 GUIDES = 3
-GUIDE_SCALE = np.array([64.0, 16.0, 1.0])
+GUIDE_SCALE = np.array([4.0, 1.0, 0.05])
 BANDWIDTH_MAX = 20.0
 
 
@@ -31,8 +31,8 @@ def bf16(x: np.ndarray) -> np.ndarray:
 
 
 def layout(n: int) -> dict:
-    nf = n + 7
-    F = nf * (2 * (n - 1) + 1)
+    nf = n + 10
+    F = nf * (2 * (n - 1) + 1) + 1
     O = (TAPS + GUIDES) * (n - 1)
     return {"n": n, "base_features": nf, "features": F, "outputs": O, "hidden": HID,
             "param_count": HID * F + HID + HID * HID + HID + O * HID + O}
@@ -64,15 +64,22 @@ def neighbour_index(screen, a: int, d: int) -> np.ndarray:
     return idx + (y - x) * stride
 
 
-def base_features(n: int, mean, var, normal, depth) -> np.ndarray:
+def base_features(n: int, screen, mean, var, normal, depth) -> np.ndarray:
     """Per-pixel base features (float32): mean (3), standard deviation of the mean (3), normal (n),
-    depth / 10."""
+    depth / 10, spatial noise estimate (3): sqrt of half the mean squared difference of the mean to
+    the 2(n-1) axis neighbours (clamped at the screen's edge)."""
     mean = np.asarray(mean, np.float32).reshape(-1, 3)
     var = np.asarray(var, np.float32).reshape(-1, 3)
     normal = np.asarray(normal, np.float32).reshape(-1, n)
     depth = np.asarray(depth, np.float32).reshape(-1)
+    m64 = mean.astype(np.float64)
+    sq = np.zeros_like(m64)
+    for a in range(n - 1):
+        for d in (-1, 1):
+            sq += (m64[neighbour_index(screen, a, d)] - m64) ** 2
+    spatial = np.sqrt(sq / (4 * (n - 1))).astype(np.float32)
     return np.concatenate([mean, np.sqrt(np.maximum(var, 0)).astype(np.float32), normal,
-                           (depth * np.float32(0.1))[:, None]], axis=1)
+                           (depth * np.float32(0.1))[:, None], spatial], axis=1)
 
 
 def guide_distances(base: np.ndarray, n: int, q: np.ndarray) -> np.ndarray:
@@ -91,14 +98,16 @@ def guide_distances(base: np.ndarray, n: int, q: np.ndarray) -> np.ndarray:
     return np.stack([dn, dd, dc], axis=1)
 
 
-def features(n: int, screen, mean, var, normal, depth) -> np.ndarray:
-    """Network input per pixel: base features (mean, std of the mean, normal, depth / 10) at the pixel
-    and at its -1 / +1 neighbours along each screen axis, in that order."""
-    base = base_features(n, mean, var, normal, depth)
+def features(n: int, screen, mean, var, normal, depth, spp: int) -> np.ndarray:
+    """Network input per pixel: base features (mean, std of the mean, normal, depth / 10, spatial
+    noise) at the pixel and at its -1 / +1 neighbours along each screen axis, in that order, then the
+    input's noise level 1 / sqrt(spp)."""
+    base = base_features(n, screen, mean, var, normal, depth)
     cols = [base]
     for a in range(n - 1):
         cols.append(base[neighbour_index(screen, a, -1)])
         cols.append(base[neighbour_index(screen, a, 1)])
+    cols.append(np.full((base.shape[0], 1), 1.0 / np.sqrt(float(spp)), np.float32))
     return np.concatenate(cols, axis=1).astype(np.float32)
 
 
@@ -108,11 +117,12 @@ def _softmax(z: np.ndarray) -> np.ndarray:
     return e / e.sum(axis=1, keepdims=True)
 
 
-def forward(params: np.ndarray, n: int, screen, mean, var, normal, depth, bf16_points: bool = True) -> dict:
+def forward(params: np.ndarray, n: int, screen, mean, var, normal, depth, *, spp: int,
+            bf16_points: bool = True) -> dict:
     """Denoised image and the intermediate values the backward pass needs."""
     p = split(params, n)
     r = bf16 if bf16_points else (lambda x: np.asarray(x, np.float64))
-    X = r(features(n, screen, mean, var, normal, depth)).astype(np.float64)
+    X = r(features(n, screen, mean, var, normal, depth, spp)).astype(np.float64)
     if bf16_points:
         W1, W2, W3 = (bf16(p[k].astype(np.float32)).astype(np.float64) for k in ("W1", "W2", "W3"))
     else:
@@ -122,7 +132,7 @@ def forward(params: np.ndarray, n: int, screen, mean, var, normal, depth, bf16_p
     H2 = np.maximum(H1 @ W2.T + p["b2"], 0)
     H2 = r(H2.astype(np.float32)).astype(np.float64) if bf16_points else H2
     Z = H2 @ W3.T + p["b3"]
-    base = base_features(n, mean, var, normal, depth)
+    base = base_features(n, screen, mean, var, normal, depth)
     A = n - 1
     ys = [np.asarray(mean, np.float64).reshape(-1, 3)]
     ws, Ds, ss = [], [], []
@@ -144,11 +154,11 @@ def forward(params: np.ndarray, n: int, screen, mean, var, normal, depth, bf16_p
             "ss": ss, "out": ys[-1]}
 
 
-def loss_and_grad(params: np.ndarray, n: int, screen, mean, var, normal, depth, target,
+def loss_and_grad(params: np.ndarray, n: int, screen, mean, var, normal, depth, target, *, spp: int,
                   bf16_points: bool = True) -> tuple[float, np.ndarray]:
     """Loss sum((out - target)^2) / sum((noisy mean - target)^2) and its gradient (flat, parameter
     order)."""
-    f = forward(params, n, screen, mean, var, normal, depth, bf16_points)
+    f = forward(params, n, screen, mean, var, normal, depth, spp=spp, bf16_points=bf16_points)
     r = (lambda x: bf16(np.asarray(x, np.float32)).astype(np.float64)) if bf16_points else (lambda x: x)
     t = np.asarray(target, np.float64).reshape(-1, 3)
     S = ((f["ys"][0] - t) ** 2).sum()

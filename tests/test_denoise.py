@@ -12,6 +12,8 @@ import pytest
 
 from oracle import denoise_oracle as dor
 
+SPP = 4  # samples per pixel the random inputs claim (the network's noise-level input is 1/2)
+
 
 def _random_inputs(n, screen, rng):
     P = int(np.prod(screen))
@@ -33,7 +35,7 @@ def _random_params(n, rng, scale=0.3):
     parts["b1"] = np.abs(parts["b1"]) * 0.1
     parts["b2"] = np.abs(parts["b2"]) * 0.1
     # guide bandwidths of a few units: every guide changes the tap weights without saturating them
-    parts["b3"][_bandwidth_columns(n)] += np.tile([-3.5, -2.5, 0.0], n - 1)
+    parts["b3"][_bandwidth_columns(n)] += np.tile([-0.75, 0.25, 3.0], n - 1)
     return dor.join(parts)
 
 
@@ -64,7 +66,7 @@ def test_oracle_backward_matches_finite_differences(n, screen):
     rng = np.random.default_rng(10 + n)
     mean, var, normal, depth, target = _random_inputs(n, screen, rng)
     params = _random_params(n, rng)
-    loss, grad = dor.loss_and_grad(params, n, screen, mean, var, normal, depth, target, bf16_points=False)
+    loss, grad = dor.loss_and_grad(params, n, screen, mean, var, normal, depth, target, spp=SPP, bf16_points=False)
     assert loss > 0
     L = dor.layout(n)
     idx = rng.choice(L["param_count"], 48, replace=False)
@@ -79,8 +81,8 @@ def test_oracle_backward_matches_finite_differences(n, screen):
         p2 = params.copy()
         p1[i] += eps
         p2[i] -= eps
-        l1, _ = dor.loss_and_grad(p1, n, screen, mean, var, normal, depth, target, bf16_points=False)
-        l2, _ = dor.loss_and_grad(p2, n, screen, mean, var, normal, depth, target, bf16_points=False)
+        l1, _ = dor.loss_and_grad(p1, n, screen, mean, var, normal, depth, target, spp=SPP, bf16_points=False)
+        l2, _ = dor.loss_and_grad(p2, n, screen, mean, var, normal, depth, target, spp=SPP, bf16_points=False)
         fd = (l1 - l2) / (2 * eps)
         assert abs(fd - grad[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, grad[i])
 
@@ -90,7 +92,7 @@ def test_oracle_uniform_filter_is_a_box_blur():
     rng = np.random.default_rng(3)
     mean, var, normal, depth, _ = _random_inputs(n, screen, rng)
     params = _box_params(n)
-    out = dor.forward(params, n, screen, mean, var, normal, depth, bf16_points=False)["out"]
+    out = dor.forward(params, n, screen, mean, var, normal, depth, spp=SPP, bf16_points=False)["out"]
     # interior pixel: mean of the 9 x 9 neighbourhood (separable, clamped at the border)
     x0, x1 = 3, 3
     img = mean.reshape(screen[1], screen[0], 3).astype(np.float64)
@@ -101,8 +103,9 @@ def test_oracle_uniform_filter_is_a_box_blur():
 
 
 def test_oracle_normal_guide_keeps_edges():
-    """Two half-screens of different normal: with tap logits 0 and the normal guide at its base
-    bandwidth (64 per unit of squared normal difference), each half is averaged over itself only."""
+    """Two half-screens of different normal: with tap logits 0 and the normal guide at 64 per unit of
+    squared normal difference (log-bandwidth ln 16 over its base 4), each half is averaged over
+    itself only."""
     n, screen = 3, (12, 5)
     P = screen[0] * screen[1]
     x0 = np.arange(P) % screen[0]
@@ -114,9 +117,9 @@ def test_oracle_normal_guide_keeps_edges():
     depth = np.full(P, 8.0, np.float32)
     params = _box_params(n)
     parts = dor.split(params.copy(), n)
-    parts["b3"][_bandwidth_columns(n)[0::dor.GUIDES]] = 0.0  # normal guide on, at 64
-    out = dor.forward(dor.join(parts), n, screen, mean, var, normal, depth, bf16_points=False)["out"]
-    box = dor.forward(params, n, screen, mean, var, normal, depth, bf16_points=False)["out"]
+    parts["b3"][_bandwidth_columns(n)[0::dor.GUIDES]] = np.log(16.0)  # normal guide on, at 64
+    out = dor.forward(dor.join(parts), n, screen, mean, var, normal, depth, spp=SPP, bf16_points=False)["out"]
+    box = dor.forward(params, n, screen, mean, var, normal, depth, spp=SPP, bf16_points=False)["out"]
     # |n_l - n_r|^2 = 0.4: every tap across the edge is weighted exp(-25.6) against the same side
     for side, level in ((left, 0.2), (~left, 0.7)):
         assert np.abs(out[side] - level).max() < 0.05
@@ -166,13 +169,13 @@ def test_forward_loss_and_gradients_match_oracle(require_gpu, n, screen):
     den = Denoiser(n, seed=5)
     params = _random_params(n, np.random.default_rng(n)).astype(np.float32)
     den.set_params(params)
-    den.set_input(screen, t["mean"], t["var"], t["normal"], t["depth"])
+    den.set_input(screen, t["mean"], t["var"], t["normal"], t["depth"], SPP)
     out = den.apply().cpu().numpy()
-    ref = dor.forward(params, n, screen, mean, var, normal, depth, bf16_points=True)
+    ref = dor.forward(params, n, screen, mean, var, normal, depth, spp=SPP, bf16_points=True)
     rel = np.linalg.norm(out - ref["out"]) / np.linalg.norm(ref["out"])
     assert rel < 2e-3, rel
     loss, grad = den.gradient(t["target"])
-    loss_o, grad_o = dor.loss_and_grad(params, n, screen, mean, var, normal, depth, target, bf16_points=True)
+    loss_o, grad_o = dor.loss_and_grad(params, n, screen, mean, var, normal, depth, target, spp=SPP, bf16_points=True)
     assert abs(loss - loss_o) <= 2e-3 * loss_o, (loss, loss_o)
     gp = dor.split(grad, n)
     go = dor.split(grad_o, n)
