@@ -262,6 +262,17 @@ int nt_accum_read_srgb_slice(nt_scene* scene, const int32_t* slice, uint32_t* ou
  * the reference, whose scene lives in host memory. */
 int nt_scene_upload(nt_scene* scene, int64_t* bytes);
 
+/* The same upload, double-buffered, so that the next frame's data cross PCIe while the current frame
+ * renders.  nt_scene_upload_begin queues the copy of the pinned host copy into a device staging
+ * buffer (one per mesh, allocated at the first call, the size of the mesh's arrays) on the scene's own
+ * copy stream and returns at once; *bytes: host-to-device bytes queued.  nt_scene_upload_commit makes
+ * the scene's stream wait for that copy and then copies the staged arrays into the live ones (device
+ * to device), so that the next nt_render on the scene's stream sees them; it fails with NT_ESTATE
+ * without a begin since the last commit, or when the scene was built in between.  A begin waits on
+ * the GPU for the previous commit's copies out of staging.  No counterpart in the reference. */
+int nt_scene_upload_begin(nt_scene* scene, int64_t* bytes);
+int nt_scene_upload_commit(nt_scene* scene);
+
 /* The scene's CUDA stream (cudaStream_t), on which nt_render and nt_trace_closest launch. */
 void* nt_scene_stream(nt_scene* scene);
 

@@ -238,6 +238,8 @@ struct MeshHost
         std::vector<int32_t> ntype;  // per facet: NormalType and reversed-vertex bits (MeshDev::ntype)
         DevBuf d_rec32, d_rec64, d_nodes, d_idx;
         DevBuf d_normals, d_fnormals, d_ntype;
+        // device staging copy of the four arrays (nt_scene_upload_begin / _commit)
+        DevBuf d_stage;
         // pinned host copy of the four device arrays, back to back (re-upload, nt_scene_upload)
         void* pinned = nullptr;
         size_t pinned_bytes = 0;
@@ -258,7 +260,7 @@ struct MeshHost
                   degenerate(o.degenerate), build_seconds(o.build_seconds), ntype(std::move(o.ntype)),
                   d_rec32(std::move(o.d_rec32)), d_rec64(std::move(o.d_rec64)), d_nodes(std::move(o.d_nodes)),
                   d_idx(std::move(o.d_idx)), d_normals(std::move(o.d_normals)), d_fnormals(std::move(o.d_fnormals)),
-                  d_ntype(std::move(o.d_ntype)),
+                  d_ntype(std::move(o.d_ntype)), d_stage(std::move(o.d_stage)),
                   pinned(o.pinned), pinned_bytes(o.pinned_bytes), ready(o.ready), uploaded(o.uploaded)
         {
                 o.pinned = nullptr;
@@ -332,9 +334,29 @@ struct nt_scene
         unsigned long long* host_counters = nullptr;
         long long samples_done = 0;
         std::vector<unsigned char> dev_scene;  // packed DevScene<N>
+        // double-buffered upload: the copy stream fills the meshes' staging buffers; `staged` marks the
+        // end of that copy, `consumed` the end of the device copies out of staging
+        cudaStream_t copy_stream = nullptr;
+        cudaEvent_t staged = nullptr;
+        cudaEvent_t consumed = nullptr;
+        bool consumed_recorded = false;
+        bool upload_staged = false;
 
         ~nt_scene()
         {
+                if (copy_stream)
+                {
+                        cudaStreamSynchronize(copy_stream);
+                        cudaStreamDestroy(copy_stream);
+                }
+                if (staged)
+                {
+                        cudaEventDestroy(staged);
+                }
+                if (consumed)
+                {
+                        cudaEventDestroy(consumed);
+                }
                 if (host_counters)
                 {
                         cudaFreeHost(host_counters);
@@ -2041,6 +2063,12 @@ int nt_scene_build(nt_scene* scene, const nt_build_opts* opts)
                 bool tree_on_gpu = opts && opts->tree_on_gpu;
                 scene->built = false;
                 scene->built_host = false;
+                // an upload staged before the build is of the old scene: a commit now is refused
+                scene->upload_staged = false;
+                if (scene->copy_stream)
+                {
+                        check_cuda(cudaStreamSynchronize(scene->copy_stream), "sync");
+                }
                 dispatch<BuildF>(scene->n, scene, threads, host_only, tree_on_gpu);
         });
 }
@@ -2135,6 +2163,82 @@ int nt_scene_upload(nt_scene* scene, int64_t* bytes)
                 {
                         *bytes = total;
                 }
+        });
+}
+
+int nt_scene_upload_begin(nt_scene* scene, int64_t* bytes)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!scene->copy_stream)
+                {
+                        check_cuda(cudaStreamCreateWithFlags(&scene->copy_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+                        check_cuda(cudaEventCreateWithFlags(&scene->staged, cudaEventDisableTiming), "cudaEventCreate");
+                        check_cuda(cudaEventCreateWithFlags(&scene->consumed, cudaEventDisableTiming), "cudaEventCreate");
+                }
+                // the previous commit's device copies still read the staging buffers
+                if (scene->consumed_recorded)
+                {
+                        check_cuda(cudaStreamWaitEvent(scene->copy_stream, scene->consumed, 0), "wait");
+                }
+                int64_t total = 0;
+                for (auto& m : scene->meshes)
+                {
+                        const size_t b = m.d_rec32.bytes + m.d_rec64.bytes + m.d_nodes.bytes + m.d_idx.bytes;
+                        if (m.d_stage.bytes != b)
+                        {
+                                // a resize frees the old buffer: nothing may still use it
+                                check_cuda(cudaStreamSynchronize(scene->copy_stream), "sync");
+                                check_cuda(cudaStreamSynchronize(scene->stream), "sync");
+                                m.d_stage.alloc(b);
+                        }
+                        if (b)
+                        {
+                                check_cuda(cudaMemcpyAsync(m.d_stage.p, m.pinned, b, cudaMemcpyHostToDevice, scene->copy_stream),
+                                           "upload");
+                        }
+                        total += (int64_t)b;
+                }
+                check_cuda(cudaEventRecord(scene->staged, scene->copy_stream), "record");
+                scene->upload_staged = true;
+                if (bytes)
+                {
+                        *bytes = total;
+                }
+        });
+}
+
+int nt_scene_upload_commit(nt_scene* scene)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!scene->upload_staged)
+                {
+                        fail(NT_ESTATE, "no staged upload (nt_scene_upload_begin)");
+                }
+                check_cuda(cudaStreamWaitEvent(scene->stream, scene->staged, 0), "wait");
+                for (auto& m : scene->meshes)
+                {
+                        const char* p = static_cast<const char*>(m.d_stage.p);
+                        DevBuf* bufs[4] = {&m.d_rec32, &m.d_rec64, &m.d_nodes, &m.d_idx};
+                        size_t off = 0;
+                        for (DevBuf* b : bufs)
+                        {
+                                if (off + b->bytes > m.d_stage.bytes)
+                                {
+                                        fail(NT_ESTATE, "the scene changed since nt_scene_upload_begin");
+                                }
+                                if (b->bytes)
+                                {
+                                        check_cuda(cudaMemcpyAsync(b->p, p + off, b->bytes, cudaMemcpyDeviceToDevice, scene->stream),
+                                                   "commit");
+                                }
+                                off += b->bytes;
+                        }
+                }
+                check_cuda(cudaEventRecord(scene->consumed, scene->stream), "record");
+                scene->consumed_recorded = true;
+                scene->upload_staged = false;
         });
 }
 

@@ -33,7 +33,7 @@ EXPORTED_SYMBOLS = (
     "nt_scene_set_projector", "nt_scene_set_background", "nt_scene_build", "nt_scene_mesh_info", "nt_render",
     "nt_accum_clear", "nt_accum_read", "nt_scene_pixel_count", "nt_trace_closest", "nt_trace_closest_device",
     "nt_scene_tree_export", "nt_last_error_message", "nt_effective_spp", "nt_cosine_sphere_coefficient",
-    "nt_scene_upload", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_add_obj_file", "nt_scene_dimension",
+    "nt_scene_upload", "nt_scene_upload_begin", "nt_scene_upload_commit", "nt_scene_stream", "nt_scene_set_mesh_normals", "nt_scene_add_obj_file", "nt_scene_dimension",
     "nt_scene_object_count", "nt_accum_read_srgb_slice", "nt_convex_hull", "nt_hull_facet_count", "nt_hull_facets",
     "nt_hull_destroy", "nt_scene_clear_lights", "nt_render_batch",
     "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
@@ -126,6 +126,8 @@ def library() -> ctypes.CDLL:
         "nt_accum_read": ([vp, f32p, ctypes.POINTER(i64)], ctypes.c_int),
         "nt_scene_pixel_count": ([vp], i64),
         "nt_scene_upload": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "nt_scene_upload_begin": ([vp, ctypes.POINTER(i64)], ctypes.c_int),
+        "nt_scene_upload_commit": ([vp], ctypes.c_int),
         "nt_scene_stream": ([vp], vp),
         "nt_trace_closest": ([vp, ctypes.c_int, f32p, f32p, i64, ctypes.c_int, i32p, f32p, ctypes.POINTER(Stats)],
                              ctypes.c_int),
@@ -336,6 +338,17 @@ class Scene:
         b = ctypes.c_int64()
         _check(self._lib.nt_scene_upload(self._h, ctypes.byref(b)))
         return int(b.value)
+
+    def upload_begin(self) -> int:
+        """Queues the copy of the scene's arrays into the device staging buffers on the scene's copy
+        stream (overlapping a render in flight); returns the bytes queued."""
+        b = ctypes.c_int64()
+        _check(self._lib.nt_scene_upload_begin(self._h, ctypes.byref(b)))
+        return int(b.value)
+
+    def upload_commit(self) -> None:
+        """Moves the staged arrays into the live ones, ordered before the next render."""
+        _check(self._lib.nt_scene_upload_commit(self._h))
 
     def render(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None,

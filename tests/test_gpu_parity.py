@@ -225,6 +225,39 @@ def test_progressive_passes_accumulate(require_gpu):
     assert rrmse(img, first) > 1e-4
 
 
+def test_double_buffered_upload_renders_the_same_scene(require_gpu):
+    """A staged upload (copy stream, then device-to-device into the live arrays) leaves the scene as
+    it was: renders of one seed before, during (the next frame's copy in flight) and after agree; a
+    commit without a begin, or after a rebuild, is refused."""
+    from math_b200 import ntrace, scenes
+
+    spec = scenes.config("n4_small")
+    s = scenes.build_scene(spec)
+    s.render(8, max_depth=5, seed=5)
+    before, _ = s.image()
+    assert s.upload_begin() > 0
+    s.upload_commit()
+    s.upload_begin()  # in flight during the next render
+    s.clear()
+    s.render(8, max_depth=5, seed=5)
+    during, _ = s.image()
+    s.upload_commit()
+    s.clear()
+    s.render(8, max_depth=5, seed=5)
+    after, _ = s.image()
+    # FP64 atomics in another order: equal to rounding
+    np.testing.assert_allclose(during, before, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(after, before, rtol=1e-9, atol=1e-12)
+    with pytest.raises(ntrace.NtraceError) as e:
+        s.upload_commit()
+    assert e.value.code == ntrace.NT_ESTATE
+    s.upload_begin()
+    s.build()
+    with pytest.raises(ntrace.NtraceError) as e:
+        s.upload_commit()
+    assert e.value.code == ntrace.NT_ESTATE
+
+
 def test_render_rejects_bad_options_and_stops(require_gpu):
     import ctypes
 
