@@ -284,7 +284,7 @@ def main() -> None:
     # step k renders, then moves into the live arrays on the device), every step's image is read back;
     # wall clock around the calls, the first step's copy included
     scene.clear()
-    e2e_steps = max(1, min(args.steps, 5))
+    e2e_steps = max(1, args.steps)
     h2d = d2h = 0
     host_img = torch.empty((scene.pixel_count, 3), dtype=torch.float32, pin_memory=True).numpy()
     torch.cuda.synchronize()
