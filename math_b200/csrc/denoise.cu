@@ -1,15 +1,14 @@
 // Learned kernel-predicting denoiser (include/ntrace_denoise.h) on the sm_100a tensor cores.
 //
-// The network's matrix products run on tcgen05: operand tiles are staged by the CTA's threads into
-// shared memory in the canonical K-major layout without swizzle (8 x 16-byte core matrices), one
-// elected thread issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in tensor memory) and
-// commits to an mbarrier, and the epilogue reads the accumulator back with tcgen05.ld.  The forward
-// pass is one persistent kernel (k_mlp_forward) that chains the three layers of a 128-pixel tile
-// through tensor and shared memory with the weights resident in shared memory; the backward data
-// products and the weight gradients (a reduction over pixels, split across CTAs) use one GEMM kernel
-// (k_gemm) whose operand loaders read row-major or transposed matrices and whose epilogues apply the
-// ReLU mask or an atomic reduction.  The rest (features, softmax filters, loss, bias sums, Adam) are
-// plain CUDA-core kernels.
+// The network's matrix products run in one GEMM kernel built on tcgen05: operand tiles are staged
+// by the CTA's threads into shared memory in the canonical K-major layout without swizzle (8 x 16-byte
+// core matrices), one elected thread issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in
+// tensor memory) and commits to an mbarrier, and the epilogue reads the accumulator back with
+// tcgen05.ld and applies a fused bias / ReLU / mask / store or atomic reduction.  Operand loaders
+// gather from any layout (row-major, transposed, or the feature stencil computed on the fly), so the
+// forward pass, the backward data products and the weight gradients (a reduction over pixels, split
+// across CTAs) all use the same kernel.  The rest (features, softmax filters, loss, bias sums, Adam)
+// are plain CUDA-core kernels.
 #include "ntrace.h"
 #include "ntrace_denoise.h"
 
@@ -407,9 +406,45 @@ struct EpiStoreF32
         }
 };
 
-// backward through ReLU: keep the gradient where the layer's output was positive; a row's 16 columns
-// are read and stored as 16-byte words (act and out 16-byte aligned, ld a multiple of 16: the hidden
-// matrices have 64 columns)
+// The epilogues below store a row's 16 columns as 16-byte words: out 16-byte aligned and ld a
+// multiple of 16 (every matrix they write has 64 or outputs_padded columns).
+struct EpiBiasF32
+{
+        const float* bias;
+        float* out;
+        int ld;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+                float4* o = reinterpret_cast<float4*>(out + (size_t)row * ld + c0);
+#pragma unroll
+                for (int j = 0; j < 4; ++j)
+                {
+                        o[j] = make_float4(v[4 * j] + bias[c0 + 4 * j], v[4 * j + 1] + bias[c0 + 4 * j + 1],
+                                           v[4 * j + 2] + bias[c0 + 4 * j + 2], v[4 * j + 3] + bias[c0 + 4 * j + 3]);
+                }
+        }
+};
+
+struct EpiBiasReluBF16
+{
+        const float* bias;
+        __nv_bfloat16* out;
+        int ld;
+        __device__ __forceinline__ void operator()(int row, int c0, const float* v) const
+        {
+                __align__(16) __nv_bfloat16 h[16];
+#pragma unroll
+                for (int j = 0; j < 16; ++j)
+                {
+                        h[j] = __float2bfloat16_rn(fmaxf(v[j] + bias[c0 + j], 0.0f));
+                }
+                uint4* o = reinterpret_cast<uint4*>(out + (size_t)row * ld + c0);
+                o[0] = reinterpret_cast<const uint4*>(h)[0];
+                o[1] = reinterpret_cast<const uint4*>(h)[1];
+        }
+};
+
+// backward through ReLU: keep the gradient where the layer's output was positive
 struct EpiMaskBF16
 {
         const __nv_bfloat16* act;
@@ -503,284 +538,6 @@ cudaError_t gemm(const LA& la, const LB& lb, const EPI& epi, int M, int N, int K
         const int kpc = k_per_cta > 0 ? (k_per_cta + GK - 1) / GK * GK : (K + GK - 1) / GK * GK;
         dim3 grid((unsigned)((M + GM - 1) / GM), (unsigned)((K + kpc - 1) / kpc));
         k_gemm<LA, LB, EPI><<<grid, GTHREADS, smem, st>>>(la, lb, epi, M, N, K, kpc, ncols, err);
-        return cudaGetLastError();
-}
-
-// ------------------------------------------------------------------------------------------------
-// Fused forward pass: the three layers of one 128-pixel tile in one CTA, chained through tensor and
-// shared memory.  The CTA is persistent: it stages the three weight matrices into shared memory once,
-// then for each of its tiles loads the input rows (16-byte loads), runs layer 1 on the tensor core
-// into tensor-memory columns 0..63, reads them back (bias, ReLU, BF16) into shared memory as the
-// next layer's A operand, layer 2 into columns 64..127, the same again, and layer 3 into columns
-// 0..outputs-1, whose epilogue adds the bias and stores the FP32 filter parameters.  H1 and H2 never
-// leave the SM unless the training pass asks for them (hidden != null).
-
-constexpr int FT = 128;  // rows per tile (the MMA's M), one per thread in the epilogues
-
-// byte offset of element (r, k) of a K-major matrix of `rows` rows stored as 64-wide K chunks, each
-// chunk in the layout of tile_off and rows x 128 bytes long: a matrix of K columns takes
-// rows x kpad64(K) x 2 bytes, the last chunk whole even when K is not a multiple of 64
-__device__ __forceinline__ uint32_t kmaj_off(int r, int k, int rows)
-{
-        return (uint32_t)((k >> 6) * rows * 128) + tile_off(r, k & 63);
-}
-
-__host__ __device__ constexpr int kpad64(int k)
-{
-        return (k + 63) / 64 * 64;
-}
-
-// rows x K BF16 row-major (leading dimension ld) into the chunked K-major layout; K a multiple of 8;
-// rows past `valid` are zero
-__device__ __forceinline__ void stage_rows(unsigned char* dst, const __nv_bfloat16* __restrict__ src, int ld, int rows,
-                                           int valid, int K)
-{
-        const int chunks = K / 8;
-        for (int idx = threadIdx.x; idx < rows * chunks; idx += blockDim.x)
-        {
-                const int r = (idx & 7) | ((idx / (8 * chunks)) << 3);
-                const int k8 = ((idx >> 3) % chunks) * 8;
-                uint4 v = make_uint4(0u, 0u, 0u, 0u);
-                if (r < valid)
-                {
-                        v = __ldg(reinterpret_cast<const uint4*>(src + (size_t)r * ld + k8));
-                }
-                *reinterpret_cast<uint4*>(dst + kmaj_off(r, k8, rows)) = v;
-        }
-}
-
-// One thread issues the MMAs of C[128 x N] (tensor memory at tmem) = A[128 x K] B[N x K]^T from the
-// chunked K-major operands and commits them to the mbarrier.
-__device__ __forceinline__ void mma_chain(uint32_t tmem, const unsigned char* A, const unsigned char* B, int N, int K,
-                                          unsigned long long* bar)
-{
-        const uint32_t idesc = umma_idesc_bf16(FT, N);
-        const uint32_t sbo = GK / 8 * 128;
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        for (int kk = 0; kk < K / 16; ++kk)
-        {
-                const int c = kk >> 2, s = kk & 3;
-                const uint64_t da = umma_desc(smem_u32(A) + c * FT * 128 + s * 256, 128, sbo);
-                const uint64_t db = umma_desc(smem_u32(B) + c * N * 128 + s * 256, 128, sbo);
-                const uint32_t accumulate = kk > 0 ? 1u : 0u;
-                asm volatile(
-                        "{\n\t.reg .pred p;\n\t"
-                        "setp.ne.b32 p, %4, 0;\n\t"
-                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem),
-                        "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
-                        : "memory");
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-                     : "memory");
-}
-
-// The hidden layer's epilogue for this thread's row: 64 accumulator columns + bias, ReLU, BF16, into
-// the next layer's A operand in shared memory (and to global memory when hidden is given).
-__device__ __forceinline__ void hidden_epilogue(uint32_t taddr, const float* __restrict__ bias, unsigned char* A, int r,
-                                                long long row, long long M, __nv_bfloat16* hidden)
-{
-#pragma unroll
-        for (int c = 0; c < HID; c += 16)
-        {
-                float v[16];
-                tmem_ld16(taddr + (uint32_t)c, v);
-                __align__(16) __nv_bfloat16 h[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j)
-                {
-                        h[j] = __float2bfloat16_rn(fmaxf(v[j] + __ldg(bias + c + j), 0.0f));
-                }
-                const uint4 lo = reinterpret_cast<const uint4*>(h)[0];
-                const uint4 hi = reinterpret_cast<const uint4*>(h)[1];
-                *reinterpret_cast<uint4*>(A + kmaj_off(r, c, FT)) = lo;
-                *reinterpret_cast<uint4*>(A + kmaj_off(r, c + 8, FT)) = hi;
-                if (hidden && row < M)
-                {
-                        uint4* g = reinterpret_cast<uint4*>(hidden + row * HID + c);
-                        g[0] = lo;
-                        g[1] = hi;
-                }
-        }
-}
-
-__global__ void __launch_bounds__(FT) k_mlp_forward(const __nv_bfloat16* __restrict__ X, int Fp, long long M,
-                                                    const __nv_bfloat16* __restrict__ W1, const float* __restrict__ b1,
-                                                    const __nv_bfloat16* __restrict__ W2, const float* __restrict__ b2,
-                                                    const __nv_bfloat16* __restrict__ W3, const float* __restrict__ b3,
-                                                    int Op, float* __restrict__ Z, __nv_bfloat16* H1, __nv_bfloat16* H2,
-                                                    int* err)
-{
-        extern __shared__ __align__(1024) unsigned char g_smem[];
-        __shared__ __align__(8) unsigned long long s_bar;
-        __shared__ uint32_t s_tmem;
-        unsigned char* sW1 = g_smem;
-        unsigned char* sW2 = sW1 + HID * kpad64(Fp) * 2;
-        unsigned char* sW3 = sW2 + HID * HID * 2;
-        unsigned char* sA = sW3 + Op * HID * 2;  // FT x kpad64(max(Fp, HID)) x 2 bytes
-        const int tid = threadIdx.x;
-        const int warp = tid >> 5;
-        constexpr uint32_t NCOLS = 128;
-
-        if (warp == 0)
-        {
-                asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                             "r"(NCOLS)
-                             : "memory");
-                asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
-        }
-        if (tid == 0)
-        {
-                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)) : "memory");
-                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        }
-        stage_rows(sW1, W1, Fp, HID, HID, Fp);
-        stage_rows(sW2, W2, HID, HID, HID, HID);
-        stage_rows(sW3, W3, HID, Op, Op, HID);
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint32_t tmem = s_tmem;
-        const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
-
-        uint32_t parity = 0;
-        bool ok = true;
-        bool pending = false;
-        // waits for the commit of the last MMA chain; false (and every thread stops) after a timeout
-        auto wait_mma = [&]() {
-                const bool done = mbar_wait(&s_bar, parity);
-                ok = __syncthreads_and(done) != 0;
-                if (ok)
-                {
-                        pending = false;
-                        parity ^= 1u;
-                        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                }
-                return ok;
-        };
-        // shared-memory operands written by the threads become visible to the tensor core, and the
-        // threads' tensor-memory reads are ordered before the next MMA
-        auto to_mma = [&]() {
-                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncthreads();
-        };
-
-        const long long tiles = (M + FT - 1) / FT;
-        for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
-        {
-                const long long m0 = tile * FT;
-                const int valid = (int)min((long long)FT, M - m0);
-                const long long row = m0 + tid;
-                stage_rows(sA, X + m0 * Fp, Fp, FT, valid, Fp);
-                to_mma();
-                if (tid == 0)
-                {
-                        mma_chain(tmem, sA, sW1, HID, Fp, &s_bar);
-                }
-                pending = true;
-                if (!wait_mma())
-                {
-                        break;
-                }
-                // the input tile is consumed: H1 takes its place
-                hidden_epilogue(tmem + lane_base, b1, sA, tid, row, M, H1);
-                to_mma();
-                if (tid == 0)
-                {
-                        mma_chain(tmem + 64, sA, sW2, HID, HID, &s_bar);
-                }
-                pending = true;
-                if (!wait_mma())
-                {
-                        break;
-                }
-                hidden_epilogue(tmem + lane_base + 64, b2, sA, tid, row, M, H2);
-                to_mma();
-                if (tid == 0)
-                {
-                        mma_chain(tmem, sA, sW3, Op, HID, &s_bar);
-                }
-                pending = true;
-                if (!wait_mma())
-                {
-                        break;
-                }
-                for (int c = 0; c < Op; c += 16)
-                {
-                        float v[16];
-                        tmem_ld16(tmem + lane_base + (uint32_t)c, v);
-                        if (row < M)
-                        {
-                                float4* o = reinterpret_cast<float4*>(Z + row * Op + c);
-#pragma unroll
-                                for (int j = 0; j < 4; ++j)
-                                {
-                                        o[j] = make_float4(v[4 * j] + __ldg(b3 + c + 4 * j), v[4 * j + 1] + __ldg(b3 + c + 4 * j + 1),
-                                                           v[4 * j + 2] + __ldg(b3 + c + 4 * j + 2),
-                                                           v[4 * j + 3] + __ldg(b3 + c + 4 * j + 3));
-                                }
-                        }
-                }
-                // the next tile overwrites sA and the accumulator columns
-                asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-                __syncthreads();
-        }
-        if (!ok && pending)
-        {
-                // a commit that did not arrive in time: wait once more (bounded) before the columns
-                // are given back
-                mbar_wait(&s_bar, parity);
-        }
-        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-        __syncthreads();
-        if (warp == 0)
-        {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
-        }
-        if (!ok && tid == 0 && err)
-        {
-                atomicOr(err, 1);
-        }
-}
-
-// Launch of the fused forward pass: one CTA per SM share of tensor memory (128 columns each, so at
-// most 4 per SM: the shared-memory request keeps it there), persistent over the tiles.
-cudaError_t mlp_forward(const __nv_bfloat16* X, int Fp, long long M, const __nv_bfloat16* W1, const float* b1,
-                        const __nv_bfloat16* W2, const float* b2, const __nv_bfloat16* W3, const float* b3, int Op,
-                        float* Z, __nv_bfloat16* H1, __nv_bfloat16* H2, int* err, cudaStream_t st)
-{
-        if (M <= 0)
-        {
-                return cudaSuccess;
-        }
-        if (Fp % 16 != 0 || Op % 16 != 0 || Op < 16 || Op > 64 || ((uintptr_t)X & 15u) || ((uintptr_t)Z & 15u))
-        {
-                return cudaErrorInvalidValue;
-        }
-        // whole 64-wide K chunks (kmaj_off): W1, W2, W3, then the tile (input rows, then H1, H2)
-        const size_t need = (size_t)(HID * kpad64(Fp) + HID * HID + Op * HID + FT * kpad64(std::max(Fp, HID))) * 2;
-        const size_t smem = std::max(need, (size_t)(SM_SMEM / 5 + 1024));
-        if (smem > 227 * 1024)
-        {
-                return cudaErrorInvalidValue;
-        }
-        cudaError_t e = cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess)
-        {
-                return e;
-        }
-        int dev = 0, sms = 0, per_sm = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_mlp_forward, FT, smem);
-        if (e != cudaSuccess)
-        {
-                return e;
-        }
-        const long long tiles = (M + FT - 1) / FT;
-        const long long grid = std::min<long long>(tiles, (long long)std::max(1, sms) * std::max(1, std::min(per_sm, 4)));
-        k_mlp_forward<<<(unsigned)grid, FT, smem, st>>>(X, Fp, M, W1, b1, W2, b2, W3, b3, Op, Z, H1, H2, err);
         return cudaGetLastError();
 }
 
@@ -1314,9 +1071,8 @@ void check_err(nt_denoiser* d)
         }
 }
 
-// forward pass of the current input: Y[n-1] is the denoised image; keep_hidden stores H1 and H2 for
-// the backward pass
-void forward(nt_denoiser* d, bool keep_hidden)
+// forward pass of the current input: Y[n-1] is the denoised image
+void forward(nt_denoiser* d)
 {
         if (d->P <= 0)
         {
@@ -1327,13 +1083,18 @@ void forward(nt_denoiser* d, bool keep_hidden)
                 pack(d);
         }
         const long long P = d->P;
+        const int P32 = (int)P;
         cudaStream_t s = d->st_use;
         int* err = d->err.as<int>();
-        ck(mlp_forward(d->X.as<__nv_bfloat16>(), d->Fp, P, d->W1.as<__nv_bfloat16>(), d->b1.as<float>(),
-                       d->W2.as<__nv_bfloat16>(), d->b2.as<float>(), d->W3.as<__nv_bfloat16>(), d->b3.as<float>(), d->Op,
-                       d->Z.as<float>(), keep_hidden ? d->H1.as<__nv_bfloat16>() : nullptr,
-                       keep_hidden ? d->H2.as<__nv_bfloat16>() : nullptr, err, s),
-           "forward");
+        ck(gemm(LoadRows{d->X.as<__nv_bfloat16>(), d->Fp}, LoadRows{d->W1.as<__nv_bfloat16>(), d->Fp},
+                EpiBiasReluBF16{d->b1.as<float>(), d->H1.as<__nv_bfloat16>(), HID}, P32, HID, d->Fp, 0, err, s),
+           "gemm 1");
+        ck(gemm(LoadRows{d->H1.as<__nv_bfloat16>(), HID}, LoadRows{d->W2.as<__nv_bfloat16>(), HID},
+                EpiBiasReluBF16{d->b2.as<float>(), d->H2.as<__nv_bfloat16>(), HID}, P32, HID, HID, 0, err, s),
+           "gemm 2");
+        ck(gemm(LoadRows{d->H2.as<__nv_bfloat16>(), HID}, LoadRows{d->W3.as<__nv_bfloat16>(), HID},
+                EpiBiasF32{d->b3.as<float>(), d->Z.as<float>(), d->Op}, P32, d->Op, HID, 0, err, s),
+           "gemm 3");
         for (int a = 0; a < d->n - 1; ++a)
         {
                 k_filter_fwd<<<blocks_for(P), TB, 0, s>>>(P, d->st, a, d->base.as<float>(), d->Z.as<float>(), d->Op,
@@ -1597,7 +1358,7 @@ int nt_denoiser_apply(nt_denoiser* d, float* d_out)
                 {
                         throw DError{NT_EINVAL, "null argument"};
                 }
-                forward(d, false);
+                forward(d);
                 ck(cudaMemcpyAsync(d_out, d->Y.as<float>() + (size_t)(d->n - 1) * d->P * 3, sizeof(float) * (size_t)d->P * 3,
                                    cudaMemcpyDeviceToDevice, d->st_use),
                    "copy");
@@ -1612,7 +1373,7 @@ int nt_denoiser_gradient(nt_denoiser* d, const float* d_target, float* grad, dou
                 {
                         throw DError{NT_EINVAL, "null argument"};
                 }
-                forward(d, true);
+                forward(d);
                 const double l = backward(d, d_target);
                 if (grad)
                 {
@@ -1634,7 +1395,7 @@ int nt_denoiser_train_step(nt_denoiser* d, const float* d_target, float lr, doub
                 {
                         throw DError{NT_EINVAL, "bad argument"};
                 }
-                forward(d, true);
+                forward(d);
                 const double l = backward(d, d_target);
                 ++d->adam_t;
                 const float c1 = 1.0f - std::pow(0.9f, (float)d->adam_t);
