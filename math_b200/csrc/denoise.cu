@@ -350,43 +350,44 @@ struct Stencil
                 const int y = min(max(x + d, 0), size[a] - 1);
                 return p + (long long)(y - x) * stride[a];
         }
-        // input feature k of pixel p
-        __device__ __forceinline__ float feature(const float* base, long long p, int k) const
-        {
-                if (k >= stencil_features)
-                {
-                        return k == stencil_features ? noise_level : 0.0f;
-                }
-                const int q = k / nf;
-                const int f = k - q * nf;
-                long long src = p;
-                if (q > 0)
-                {
-                        const int a = (q - 1) >> 1;
-                        src = neighbour(p, a, (q & 1) ? -1 : 1);
-                }
-                return base[src * nf + f];
-        }
 };
 
 // The network's input matrix X (pixels x padded features, BF16), written once per input: thread
-// (pixel, chunk) forms eight consecutive features and stores them as one 16-byte word, so that
-// consecutive threads write consecutive chunks of a row.
+// (pixel, slot) resolves the slot's source pixel once (the pixel, or its -1 / +1 neighbour along an
+// axis) and converts that pixel's nf base features into the row's slot; the extra last slot writes the
+// noise level and the zero padding.  Consecutive threads write consecutive runs of a row.
 __global__ void k_features(long long P, Stencil st, int Fp, const float* __restrict__ base, __nv_bfloat16* __restrict__ X)
 {
-        const int chunks = Fp / 8;
-        const long long total = P * chunks;
+        const int S = 2 * st.axes + 1;
+        const int per = S + 1;
+        const long long total = P * per;
+        const int nf = st.nf;
         for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
         {
-                const long long p = i / chunks;
-                const int c = (int)(i - p * chunks);
-                __align__(16) __nv_bfloat16 v[8];
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
+                const long long p = i / per;
+                const int q = (int)(i - p * per);
+                __nv_bfloat16* row = X + p * Fp;
+                if (q < S)
                 {
-                        v[j] = __float2bfloat16_rn(st.feature(base, p, c * 8 + j));
+                        long long src = p;
+                        if (q > 0)
+                        {
+                                src = st.neighbour(p, (q - 1) >> 1, (q & 1) ? -1 : 1);
+                        }
+                        const float* b = base + src * nf;
+                        __nv_bfloat16* o = row + q * nf;
+                        for (int f = 0; f < nf; ++f)
+                        {
+                                o[f] = __float2bfloat16_rn(__ldg(b + f));
+                        }
                 }
-                *reinterpret_cast<uint4*>(X + p * Fp + c * 8) = *reinterpret_cast<const uint4*>(v);
+                else
+                {
+                        for (int k = st.stencil_features; k < Fp; ++k)
+                        {
+                                row[k] = __float2bfloat16_rn(k == st.stencil_features ? st.noise_level : 0.0f);
+                        }
+                }
         }
 }
 
@@ -1343,8 +1344,8 @@ int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, int samples_per
                 d->G.ensure(sizeof(float) * (size_t)P * 3 * 2);
                 k_base_features<<<blocks_for(P), TB, 0, d->st_use>>>(P, st, d_mean, d_var, d_normal, d_depth,
                                                                       d->base.as<float>());
-                k_features<<<blocks_for(P * (d->Fp / 8)), TB, 0, d->st_use>>>(P, st, d->Fp, d->base.as<float>(),
-                                                                              d->X.as<__nv_bfloat16>());
+                k_features<<<blocks_for(P * (2 * st.axes + 2)), TB, 0, d->st_use>>>(P, st, d->Fp, d->base.as<float>(),
+                                                                                     d->X.as<__nv_bfloat16>());
                 ck(cudaGetLastError(), "features");
                 ck(cudaMemcpyAsync(d->Y.p, d_mean, sizeof(float) * (size_t)P * 3, cudaMemcpyDeviceToDevice, d->st_use),
                    "copy");
