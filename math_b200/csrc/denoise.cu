@@ -352,42 +352,60 @@ struct Stencil
         }
 };
 
-// The network's input matrix X (pixels x padded features, BF16), written once per input: thread
-// (pixel, slot) resolves the slot's source pixel once (the pixel, or its -1 / +1 neighbour along an
-// axis) and converts that pixel's nf base features into the row's slot; the extra last slot writes the
-// noise level and the zero padding.  Consecutive threads write consecutive runs of a row.
-__global__ void k_features(long long P, Stencil st, int Fp, const float* __restrict__ base, __nv_bfloat16* __restrict__ X)
+// Source pixel of stencil slot q of pixel p (slot 0 the pixel, 2a + 1 / 2a + 2 its -1 / +1 neighbour
+// along axis a, clamped), in 32-bit arithmetic (at most 2^30 pixels)
+__device__ __forceinline__ unsigned slot_source(const Stencil& st, unsigned p, int q)
 {
-        const int S = 2 * st.axes + 1;
-        const int per = S + 1;
-        const long long total = P * per;
+        if (q <= 0 || q > 2 * st.axes)
+        {
+                return p;
+        }
+        const int a = (q - 1) >> 1;
+        const unsigned stride = (unsigned)st.stride[a];
+        const int x = (int)((p / stride) % (unsigned)st.size[a]);
+        const int y = min(max(x + ((q & 1) ? -1 : 1), 0), st.size[a] - 1);
+        return (unsigned)((int)p + (y - x) * (int)stride);
+}
+
+// The network's input matrix X (pixels x padded features, BF16), written once per input: thread
+// (pixel, chunk) forms eight consecutive features and stores them as one 16-byte word, so that
+// consecutive threads write consecutive chunks of a row.  A chunk spans at most two stencil slots
+// (nf > 8), so the thread walks the slots incrementally: one source pixel per slot it touches.
+__global__ void k_features(long long P, __grid_constant__ const Stencil st, int Fp, const float* __restrict__ base, __nv_bfloat16* __restrict__ X)
+{
+        const int chunks = Fp / 8;
+        const long long total = P * chunks;
         const int nf = st.nf;
+        const int S = 2 * st.axes + 1;
         for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
         {
-                const long long p = i / per;
-                const int q = (int)(i - p * per);
-                __nv_bfloat16* row = X + p * Fp;
-                if (q < S)
+                const unsigned p = (unsigned)(i / chunks);
+                const int c = (int)(i - (long long)p * chunks);
+                int q = (c * 8) / nf;
+                int f = c * 8 - q * nf;
+                unsigned src = slot_source(st, p, q);
+                __align__(16) __nv_bfloat16 v[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
                 {
-                        long long src = p;
-                        if (q > 0)
+                        float x = 0.0f;
+                        if (q < S)
                         {
-                                src = st.neighbour(p, (q - 1) >> 1, (q & 1) ? -1 : 1);
+                                x = __ldg(base + (size_t)src * nf + f);
                         }
-                        const float* b = base + src * nf;
-                        __nv_bfloat16* o = row + q * nf;
-                        for (int f = 0; f < nf; ++f)
+                        else if (q == S && f == 0)
                         {
-                                o[f] = __float2bfloat16_rn(__ldg(b + f));
+                                x = st.noise_level;
+                        }
+                        v[j] = __float2bfloat16_rn(x);
+                        if (++f == nf)
+                        {
+                                f = 0;
+                                ++q;
+                                src = slot_source(st, p, q);
                         }
                 }
-                else
-                {
-                        for (int k = st.stencil_features; k < Fp; ++k)
-                        {
-                                row[k] = __float2bfloat16_rn(k == st.stencil_features ? st.noise_level : 0.0f);
-                        }
-                }
+                *reinterpret_cast<uint4*>(X + (size_t)p * Fp + c * 8) = *reinterpret_cast<const uint4*>(v);
         }
 }
 
@@ -556,7 +574,7 @@ unsigned blocks_for(long long n)
 // the spatial noise estimate (3): sqrt of half the mean squared difference of the mean to the 2(n-1)
 // axis neighbours (clamped), which for independent noise over a locally constant image is the
 // standard deviation of the mean; unlike the per-pixel estimate it exists at one sample per pixel
-__global__ void k_base_features(long long P, Stencil st, const float* __restrict__ mean, const float* __restrict__ var,
+__global__ void k_base_features(long long P, __grid_constant__ const Stencil st, const float* __restrict__ mean, const float* __restrict__ var,
                                 const float* __restrict__ normal, const float* __restrict__ depth, float* __restrict__ out)
 {
         const int nf = st.nf;
@@ -685,7 +703,7 @@ __device__ __forceinline__ void tap_weights(const Stencil& st, const float* __re
 }
 
 // y_out[p] = sum_j w_j y_in[p + (j - 4) e_a] with the tap weights above
-__global__ void k_filter_fwd(long long P, Stencil st, int a, const float* __restrict__ base, const float* __restrict__ Z,
+__global__ void k_filter_fwd(long long P, __grid_constant__ const Stencil st, int a, const float* __restrict__ base, const float* __restrict__ Z,
                              int ldz, const float* __restrict__ y_in, float* __restrict__ y_out)
 {
         for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
@@ -714,7 +732,7 @@ __global__ void k_filter_fwd(long long P, Stencil st, int a, const float* __rest
 
 // backward of k_filter_fwd: dZ for the axis's tap logits and log-bandwidths (through the softmax) and,
 // when g_in is given, dL/dy_in added by atomics
-__global__ void k_filter_bwd(long long P, Stencil st, int a, const float* __restrict__ base, const float* __restrict__ Z,
+__global__ void k_filter_bwd(long long P, __grid_constant__ const Stencil st, int a, const float* __restrict__ base, const float* __restrict__ Z,
                              int ldz, const float* __restrict__ y_in, const float* __restrict__ g_out, float* g_in,
                              __nv_bfloat16* __restrict__ dZ)
 {
@@ -1344,8 +1362,8 @@ int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, int samples_per
                 d->G.ensure(sizeof(float) * (size_t)P * 3 * 2);
                 k_base_features<<<blocks_for(P), TB, 0, d->st_use>>>(P, st, d_mean, d_var, d_normal, d_depth,
                                                                       d->base.as<float>());
-                k_features<<<blocks_for(P * (2 * st.axes + 2)), TB, 0, d->st_use>>>(P, st, d->Fp, d->base.as<float>(),
-                                                                                     d->X.as<__nv_bfloat16>());
+                k_features<<<blocks_for(P * (d->Fp / 8)), TB, 0, d->st_use>>>(P, st, d->Fp, d->base.as<float>(),
+                                                                              d->X.as<__nv_bfloat16>());
                 ck(cudaGetLastError(), "features");
                 ck(cudaMemcpyAsync(d->Y.p, d_mean, sizeof(float) * (size_t)P * 3, cudaMemcpyDeviceToDevice, d->st_use),
                    "copy");
