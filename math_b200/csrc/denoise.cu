@@ -38,6 +38,9 @@ constexpr int MAX_AXES = 5;
 // tap logits is GUIDE_SCALE x exp(min(o, BANDWIDTH_MAX)).
 constexpr int GUIDES = 3;
 constexpr float BANDWIDTH_MAX = 20.0f;
+// floats per pixel in the base-feature buffer: n + 10 of them used (n <= 6), the rest zero, so that a
+// pixel's features are four aligned 16-byte words
+constexpr int BASE_STRIDE = 16;
 
 // ------------------------------------------------------------------------------------------------
 // tcgen05 GEMM
@@ -391,7 +394,7 @@ __global__ void k_features(long long P, __grid_constant__ const Stencil st, int 
                         float x = 0.0f;
                         if (q < S)
                         {
-                                x = __ldg(base + (size_t)src * nf + f);
+                                x = __ldg(base + (size_t)src * BASE_STRIDE + f);
                         }
                         else if (q == S && f == 0)
                         {
@@ -582,7 +585,7 @@ __global__ void k_base_features(long long P, __grid_constant__ const Stencil st,
         const float inv = 1.0f / (float)(4 * st.axes);
         for (long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x; p < P; p += (long long)gridDim.x * blockDim.x)
         {
-                float* o = out + p * nf;
+                float* o = out + p * BASE_STRIDE;
                 float m[3], sq[3] = {0, 0, 0};
                 for (int c = 0; c < 3; ++c)
                 {
@@ -610,6 +613,10 @@ __global__ void k_base_features(long long P, __grid_constant__ const Stencil st,
                 for (int c = 0; c < 3; ++c)
                 {
                         o[7 + n + c] = sqrtf(sq[c] * inv);
+                }
+                for (int k = nf; k < BASE_STRIDE; ++k)
+                {
+                        o[k] = 0.0f;
                 }
         }
 }
@@ -650,18 +657,38 @@ __device__ __forceinline__ float guide_scale(int g)
 // "Adaptive rendering with non-local means filtering", 2012): the squared difference of the means
 // less the variance it carries from the noise, over that variance plus a small relative floor,
 // averaged over the channels.
-__device__ __forceinline__ void guide_distance(const float* __restrict__ base, int nf, long long p, long long q, float* D)
+__device__ __forceinline__ void load_base(const float* __restrict__ base, long long p, float* b)
 {
-        const int n = nf - 10;
-        const float* bp = base + p * nf;
-        const float* bq = base + q * nf;
-        float dn = 0;
-        for (int k = 0; k < n; ++k)
+        const float4* s = reinterpret_cast<const float4*>(base + p * BASE_STRIDE);
+#pragma unroll
+        for (int i = 0; i < BASE_STRIDE / 4; ++i)
         {
-                const float t = bp[6 + k] - bq[6 + k];
-                dn += t * t;
+                const float4 t = __ldg(s + i);
+                b[4 * i] = t.x;
+                b[4 * i + 1] = t.y;
+                b[4 * i + 2] = t.z;
+                b[4 * i + 3] = t.w;
         }
-        const float dd = 10.0f * (bp[6 + n] - bq[6 + n]);
+}
+
+// bp, bq: the two pixels' base features (load_base); n: the space dimension (3..6)
+__device__ __forceinline__ void guide_distance(const float* bp, const float* bq, int n, float* D)
+{
+        float dn = 0;
+#pragma unroll
+        for (int k = 0; k < 6; ++k)
+        {
+                if (k < n)
+                {
+                        const float t = bp[6 + k] - bq[6 + k];
+                        dn += t * t;
+                }
+        }
+        // depth / 10 at 6 + n, picked by selects (an index computed from n would send the arrays to
+        // local memory)
+        const float dp = n == 3 ? bp[9] : (n == 4 ? bp[10] : (n == 5 ? bp[11] : bp[12]));
+        const float dq = n == 3 ? bq[9] : (n == 4 ? bq[10] : (n == 5 ? bq[11] : bq[12]));
+        const float dd = 10.0f * (dp - dq);
         float dc = 0;
 #pragma unroll
         for (int c = 0; c < 3; ++c)
@@ -692,11 +719,15 @@ __device__ __forceinline__ void tap_weights(const Stencil& st, const float* __re
                 s[g] = guide_scale(g) * expf(fminf(o, BANDWIDTH_MAX));
         }
         float z[TAPS];
+        float bp[BASE_STRIDE];
+        load_base(base, p, bp);
 #pragma unroll
         for (int j = 0; j < TAPS; ++j)
         {
                 q[j] = st.neighbour(p, a, j - RADIUS);
-                guide_distance(base, st.nf, p, q[j], D[j]);
+                float bq[BASE_STRIDE];
+                load_base(base, q[j], bq);
+                guide_distance(bp, bq, st.nf - 10, D[j]);
                 z[j] = zrow[a * TAPS + j] - (s[0] * D[j][0] + s[1] * D[j][1] + s[2] * D[j][2]);
         }
         softmax9(z, w);
@@ -1350,7 +1381,7 @@ int nt_denoiser_set_input(nt_denoiser* d, const int32_t* screen, int samples_per
                 d->st = st;
                 d->P = P;
                 d->st_use = stream ? (cudaStream_t)stream : d->own;
-                d->base.ensure(sizeof(float) * (size_t)P * d->nf);
+                d->base.ensure(sizeof(float) * (size_t)P * BASE_STRIDE);
                 d->X.ensure(sizeof(__nv_bfloat16) * (size_t)P * d->Fp);
                 d->H1.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
                 d->H2.ensure(sizeof(__nv_bfloat16) * (size_t)P * HID);
