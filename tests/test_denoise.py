@@ -102,6 +102,36 @@ def test_oracle_uniform_filter_is_a_box_blur():
     np.testing.assert_allclose(out[x1 * screen[0] + x0], expect, rtol=1e-12)
 
 
+def test_oracle_input_features_layout():
+    """Input row: (n + 10) base features at the pixel and its 2(n-1) axis neighbours, then the noise
+    level 1/sqrt(spp); the spatial noise estimate is 0 on a constant image and close to the noise's
+    standard deviation on independent noise."""
+    n, screen = 4, (9, 8, 7)
+    P = int(np.prod(screen))
+    rng = np.random.default_rng(21)
+    normal = np.tile([0.0, 0.0, 0.0, 1.0], (P, 1)).astype(np.float32)
+    depth = np.full(P, 8.0, np.float32)
+    var = np.zeros((P, 3), np.float32)
+    flat = np.full((P, 3), 0.4, np.float32)
+    X = dor.features(n, screen, flat, var, normal, depth, 9)
+    L = dor.layout(n)
+    nf = n + 10
+    assert X.shape == (P, L["features"]) and L["features"] == nf * (2 * (n - 1) + 1) + 1
+    np.testing.assert_array_equal(X[:, -1], np.float32(1.0 / 3.0))
+    np.testing.assert_array_equal(X[:, 7 + n:10 + n], 0.0)  # spatial noise of a constant image
+    # the -1 neighbour along axis 1 of pixel (x0, x1, x2) = (4, 3, 2) is (4, 2, 2)
+    mean = rng.uniform(0, 1, (P, 3)).astype(np.float32)
+    X = dor.features(n, screen, mean, var, normal, depth, 1)
+    p = 4 + 9 * (3 + 8 * 2)
+    q = 4 + 9 * (2 + 8 * 2)
+    np.testing.assert_array_equal(X[p, 3 * nf:3 * nf + 3], mean[q])
+    sigma = 0.05
+    noisy = (0.5 + rng.normal(0, sigma, (P, 3))).astype(np.float32)
+    spatial = dor.base_features(n, screen, noisy, var, normal, depth)[:, 7 + n:10 + n]
+    interior = spatial.reshape(screen[2], screen[1], screen[0], 3)[1:-1, 1:-1, 1:-1]
+    assert abs(float(np.sqrt((interior.astype(np.float64) ** 2).mean())) - sigma) < 0.15 * sigma
+
+
 def test_oracle_normal_guide_keeps_edges():
     """Two half-screens of different normal: with tap logits 0 and the normal guide at 64 per unit of
     squared normal difference (log-bandwidth ln 16 over its base 4), each half is averaged over
