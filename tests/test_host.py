@@ -135,6 +135,15 @@ def test_rejects_malformed_scenes():
     s5.add_mesh(v, f)
     s5.set_projector(0, (0, 0, 5), (0, 0, -1), np.eye(3)[:2], 0.1, (8, 8))
     assert _code(lambda: s5.build(host_only=True)) == NT_EINVAL
+    # a scene built for the host only has no device arrays: uploads are refused
+    s6 = ntrace.Scene(3)
+    s6.add_mesh(v, f)
+    s6.add_point_light((0, 0, 5), (1, 1, 1), 1.0)
+    s6.set_projector(0, (0, 0, 5), (0, 0, -1), np.eye(3)[:2], 0.1, (8, 8))
+    s6.build(host_only=True)
+    assert _code(lambda: s6.upload()) == NT_ESTATE
+    assert _code(lambda: s6.upload_begin()) == NT_ESTATE
+    assert _code(lambda: s6.upload_commit()) == NT_ESTATE
     # bad screen size and unknown projector kind
     assert _code(lambda: s5.set_projector(0, (0, 0, 5), (0, 0, -1), np.eye(3)[:2], 0.1, (0, 8))) == NT_EINVAL
     assert _code(lambda: s5.set_projector(5, (0, 0, 5), (0, 0, -1), np.eye(3)[:2], 0.1, (8, 8))) == NT_EINVAL
