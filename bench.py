@@ -234,10 +234,16 @@ def main() -> None:
     spp, depth = spec["spp"], spec["max_depth"]
     stream = torch.cuda.ExternalStream(scene.stream)
 
+    # the library's autotuner picks the path-pool size and the iterations per graph launch from probe
+    # passes of this frame (untimed; it clears the accumulator)
+    tuned, _ = scene.autotune(spp, max_depth=depth, seed=spec["seed"] + rank)
+    ropts = dict(max_depth=depth, seed=spec["seed"] + rank, pool_paths=tuned["pool_paths"],
+                 graph_iterations=tuned["graph_iterations"])
+
     # warm-up (also the per-kernel timing pass: device events around every launch)
     for _ in range(args.warmup - 1):
-        scene.render(spp, max_depth=depth, seed=spec["seed"] + rank)
-    timed = scene.render(spp, max_depth=depth, seed=spec["seed"] + rank, timing=True)
+        scene.render(spp, **ropts)
+    timed = scene.render(spp, **ropts, timing=True)
     scene.clear()
 
     # timed region: K frames, device time between two events on the scene's stream
@@ -250,7 +256,7 @@ def main() -> None:
         torch.cuda.synchronize()
         ev0.record(stream)
         for _ in range(args.steps):
-            stats.append(scene.render(spp, max_depth=depth, seed=spec["seed"] + rank))
+            stats.append(scene.render(spp, **ropts))
         ev1.record(stream)
         torch.cuda.synchronize()
         if dist:
@@ -295,7 +301,7 @@ def main() -> None:
         scene.upload_commit()
         if k + 1 < e2e_steps:
             scene.upload_begin()
-        st = scene.render(spp, max_depth=depth, seed=spec["seed"] + rank)
+        st = scene.render(spp, **ropts)
         scene.image(out=host_img)
         e2e_paths += st["paths"]
         d2h = host_img.nbytes
@@ -316,11 +322,18 @@ def main() -> None:
         walks[kind] = {"bytes": b / launches_k, "flops": f / launches_k, "launch_ms": ms,
                        "achieved": (b / launches_k) / (ms / 1000.0) / 1e9 if ms > 0 else 0.0}
     dom = max(walks, key=lambda k: timed[k + "_ms"])
+    # DRAM bytes per launch from an ncu capture (profiles/traffic.json), scaled by the algorithmic bytes
+    # of this run's launches over those of the captured ones when the pool size differs (a launch's
+    # traffic grows with the rays it processes)
     traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         try:
-            traffic = json.loads(tf.read_text()).get(f"{args.config}_{dom}_bytes_per_launch")
+            t = json.loads(tf.read_text())
+            traffic = t.get(f"{args.config}_{dom}_bytes_per_launch")
+            alg = t.get(f"{args.config}_{dom}_algorithmic_bytes_per_launch")
+            if traffic is not None and t.get("pool_paths") != tuned["pool_paths"]:
+                traffic = traffic * walks[dom]["bytes"] / alg if alg else None
         except Exception:
             traffic = None
     achieved = walks[dom]["achieved"]
@@ -329,7 +342,8 @@ def main() -> None:
         "metric": metric_name(n), "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": config_block(spec, args),
+        "config": dict(config_block(spec, args), pool_paths=tuned["pool_paths"],
+                       graph_iterations=tuned["graph_iterations"], tuned_by="nt_autotune"),
         "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": launches,
