@@ -2449,14 +2449,14 @@ int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tun
                 }
                 const long long total = scene->pixel_count() * (long long)nt_effective_spp(scene->n, base->samples_per_pixel);
                 std::vector<long long> pools;
-                for (long long q = 1ll << 20; q <= (1ll << 23); q <<= 1)
+                for (long long q = 1ll << 20; q <= (1ll << 24); q <<= 1)
                 {
                         if (q < 2 * total || pools.empty())
                         {
                                 pools.push_back(std::min(q, std::max<long long>(256, total)));
                         }
                 }
-                const int iters[] = {2, 4, 8};
+                const int iters[] = {2, 4, 8, 16};
                 nt_render_opts best = *base;
                 double best_t = 1e300;
                 for (long long q : pools)
