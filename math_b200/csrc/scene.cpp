@@ -2449,7 +2449,7 @@ int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tun
                 }
                 const long long total = scene->pixel_count() * (long long)nt_effective_spp(scene->n, base->samples_per_pixel);
                 std::vector<long long> pools;
-                for (long long q = 1ll << 20; q <= (1ll << 24); q <<= 1)
+                for (long long q = 1ll << 20; q <= (1ll << 25); q <<= 1)
                 {
                         if (q < 2 * total || pools.empty())
                         {
