@@ -367,6 +367,9 @@ def main() -> None:
         result["combine_ms"] = combine_ms
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(spec, args.cpu_paths, os.cpu_count() or 1)
+        # the same painter on one thread, over an eighth of the sample
+        one = cpu_baseline(spec, max(1000, args.cpu_paths // 8), 1)
+        result["cpu_baseline"]["single_thread"] = {k: one[k] for k in ("value", "unit", "cores", "kind", "sample")}
     if rank == 0:
         print(json.dumps(result))
     if dist:
