@@ -269,7 +269,9 @@ int nt_scene_upload(nt_scene* scene, int64_t* bytes);
  * the scene's stream wait for that copy and then copies the staged arrays into the live ones (device
  * to device), so that the next nt_render on the scene's stream sees them; it fails with NT_ESTATE
  * without a begin since the last commit, or when the scene was built in between.  A begin waits on
- * the GPU for the previous commit's copies out of staging.  No counterpart in the reference. */
+ * the GPU for the previous commit's copies out of staging.  The commit's copies are ordered only on
+ * the scene's stream: a render on another stream (nt_render_noalloc's) must be ordered after them by
+ * the caller (an event recorded on nt_scene_stream).  No counterpart in the reference. */
 int nt_scene_upload_begin(nt_scene* scene, int64_t* bytes);
 int nt_scene_upload_commit(nt_scene* scene);
 
