@@ -73,6 +73,12 @@ typedef struct nt_render_opts
         const volatile int* stop; /* optional host stop flag, polled between batches of wavefront iterations */
         int graph_iterations;   /* wavefront iterations per CUDA-graph launch (the host checks for the end of
                                    the pass after each); <= 0: 4.  nt_autotune picks it with pool_paths. */
+        int64_t sample_offset;  /* > 0: index of this pass's first sample per pixel (a sample range of its own,
+                                   e.g. one rank's share of a frame rendered on several GPUs: samples
+                                   [sample_offset, sample_offset + effective spp) trace the same paths whichever
+                                   process renders them); 0: continue after the samples already accumulated
+                                   (progressive passes).  The accumulator's sample count grows by the pass's
+                                   samples either way. */
 } nt_render_opts;
 
 typedef struct nt_stats
@@ -190,8 +196,19 @@ int nt_scene_mesh_info(nt_scene* scene, int mesh_index, nt_mesh_info* info);
 /* ---- painting (paint<N,T>) ---- */
 
 /* One pass: samples_per_pixel (stratified, effective count k^(n-1)) more samples for every pixel
- * of the screen, added to the scene's accumulator; successive calls continue the sample sequence. */
+ * of the screen, added to the scene's accumulator; successive calls continue the sample sequence
+ * (or start at opts->sample_offset). */
 int nt_render(nt_scene* scene, const nt_render_opts* opts, nt_stats* stats);
+
+/* paint_pixels over a list of pixels (src/painter/painter.cpp:410-448 with a Paintbrush that hands out
+ * exactly these pixels, paintbrush.h:26-233): samples_per_pixel (effective k^(n-1)) samples of each
+ * listed pixel, samples [max(opts->sample_offset, 0), + effective spp), the same paths as a whole-frame
+ * pass with that sample range traces for those pixels.  pixels: count linear pixel indices (x0 fastest,
+ * each in [0, pixel count); repeats allowed) in host memory; rgb_mean: count x 3 host floats, the mean
+ * colour of each listed pixel over the pass.  The scene's accumulator is not touched.  Used for
+ * converged-radiance checks on pixel subsets and for partial re-renders. */
+int nt_render_pixels(nt_scene* scene, const nt_render_opts* opts, const int64_t* pixels, int64_t count,
+                     float* rgb_mean, nt_stats* stats);
 
 /* nt_render for callers that cannot allocate device memory: applications that own all device memory
  * through their own allocator or a budget fixed at start-up, plugins inside such hosts, and frame
@@ -202,14 +219,24 @@ int nt_render(nt_scene* scene, const nt_render_opts* opts, nt_stats* stats);
  * memory is one file-scope device array of NT_NOALLOC_SCRATCH_BYTES inside the library, and the pass's
  * per-pixel sums (red, green, blue as doubles, x0 fastest) are ADDED to the caller's d_accum
  * (pixel_count x 3 doubles of device memory; zero it before the first pass).  sample_offset is the
- * index of the pass's first sample per pixel (0, then the effective samples of the passes before).
- * stream: a cudaStream_t, NULL for the scene's stream.  The call allocates nothing: no cudaMalloc,
- * cudaFree, cudaMallocHost, stream or event; its first call on a device looks up the array's device
- * address (cudaGetSymbolAddress) for that device, so make that first call before any stream capture.
- * The array holds at most the path pool that fits in it: opts->pool_paths above that capacity is
- * rejected with NT_EINVAL (0 uses the capacity).  Every GPU that loads the library keeps the array
- * until the process exits; all calls share it and it keeps the last call's contents (each call clears
- * its counters), so calls that overlap on the GPU race and must be serialised by the caller. */
+ * index of the pass's first sample per pixel (0, then the effective samples of the passes before);
+ * opts->sample_offset is not used here.  stream: a cudaStream_t, NULL for the scene's stream.
+ * The call allocates nothing: no cudaMalloc, cudaFree, cudaMallocHost, stream or event.  Its first
+ * call on a device does a one-time set-up for that device: it looks up the array's device address
+ * (cudaGetSymbolAddress), and under CUDA's lazy module loading (the default since CUDA 12.2) that
+ * look-up is also what loads the library's module holding the array, so the array's 64 MiB are
+ * reserved on the device then.  Make that first call (a warm-up pass) at start-up, while device
+ * memory is still available, and before any stream capture.  The array holds at most the path pool
+ * that fits in it: opts->pool_paths above that capacity is rejected with NT_EINVAL (0 uses the
+ * capacity).  The iterations are enqueued one by one with no events: opts->timing and
+ * opts->graph_iterations are ignored and the *_ms fields of stats stay 0.  Every GPU that loads the
+ * library keeps the array until the process exits; all calls share it and it keeps the last call's
+ * contents (each call clears its counters), so calls that overlap on the GPU race and must be
+ * serialised by the caller.  A stream other than the scene's must be ordered by the caller (an event
+ * recorded on nt_scene_stream) after every earlier asynchronous update of the scene's device arrays:
+ * nt_scene_build and nt_scene_upload finish theirs before they return, but nt_scene_upload_commit
+ * only enqueues its copies on the scene's stream, and so does any later call documented as
+ * asynchronous on that stream. */
 #define NT_NOALLOC_SCRATCH_BYTES (64u << 20)
 int nt_render_noalloc(nt_scene* scene, const nt_render_opts* opts, double* d_accum, int64_t sample_offset,
                       void* stream, nt_stats* stats);

@@ -154,6 +154,9 @@ struct PassDev
         int moments;              // 1: radiance is summed per path (index pixel * spp_eff + sample of
                                   // the pass) instead of per pixel; the path queues then carry that
                                   // index in place of the pixel
+        const long long* list;    // non-null: the pass paints these pixels (linear indices) only; path g
+                                  // is sample g % spp_eff of list entry g / spp_eff, and the queues carry
+                                  // the entry (the accumulator has one slot per entry)
 };
 
 // Device-wide counters (one int64 each).

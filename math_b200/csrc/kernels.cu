@@ -201,8 +201,9 @@ template <int N>
 __device__ __forceinline__ void raygen_one(const DevScene<N>& S, const PassDev& P, const PathView<N>& A, long long g,
                                            long long slot)
 {
-        long long pixel = g / P.spp_eff;
-        int s = (int)(g - pixel * P.spp_eff);
+        const long long entry = g / P.spp_eff;
+        int s = (int)(g - entry * P.spp_eff);
+        const long long pixel = P.list ? P.list[entry] : entry;
         long long sample = P.sample_offset + s;
         unsigned long long path = (unsigned long long)sample * (unsigned long long)P.npix + (unsigned long long)pixel;
 
@@ -248,7 +249,7 @@ __device__ __forceinline__ void raygen_one(const DevScene<N>& S, const PassDev& 
         A.at(2 * N + 1, slot) = 1.0f;
         A.at(2 * N + 2, slot) = 1.0f;
         A.at(2 * N + 3, slot) = 1.0f;
-        A.pix[slot] = P.moments ? (uint32_t)g : (uint32_t)pixel;
+        A.pix[slot] = P.moments ? (uint32_t)g : (uint32_t)entry;
         A.smp[slot] = (uint32_t)sample;
         A.level[slot] = 0;
 }
@@ -535,7 +536,8 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                 float nr_org[N], nr_dir[N];
                 if (lit && level < S.max_depth)
                 {
-                        const unsigned long long px = P.moments ? pixel / (uint32_t)P.spp_eff : pixel;
+                        const unsigned long long px = P.moments ? pixel / (uint32_t)P.spp_eff
+                                                                : (P.list ? (unsigned long long)P.list[pixel] : pixel);
                         unsigned long long path = (unsigned long long)sample * (unsigned long long)P.npix + px;
                         float d[N];
                         if (cosine_hemisphere<N>(P.key0, P.key1, path, (uint32_t)(1 + level), sn, d))

@@ -9,8 +9,11 @@
 // scene's arrays (built beforehand) are the inputs and the caller's accumulator is the output.
 // Nothing here calls cudaMalloc, cudaFree, cudaMallocHost, or creates a stream or an event.
 //
-// Every GPU that loads the library holds the array until the process exits.  All calls share it and
-// it keeps the previous call's contents: the counters are cleared at the start of every call, the
+// Every GPU that loads the library holds the array until the process exits.  With CUDA's lazy module
+// loading (the default since CUDA 12.2) the module holding the array is loaded, and its 64 MiB
+// reserved, by the first cudaGetSymbolAddress on a device, which the first call on that device makes:
+// callers with a fixed budget make that call once at start-up.  All calls share the array and it
+// keeps the previous call's contents: the counters are cleared at the start of every call, the
 // queues are always written before they are read, and calls that overlap on the GPU (two streams,
 // two threads) race on it.
 #include "ntrace.h"

@@ -330,7 +330,8 @@ struct nt_scene
         bool pool_smooth = false;
         DevBuf counters;
         DevBuf moments;  // per-path sums of nt_render_moments
-        DevBuf mean_buf; // mean colours for nt_accum_read
+        DevBuf mean_buf; // mean colours for nt_accum_read and nt_render_pixels
+        DevBuf list_buf; // nt_render_pixels: the pixel list, then its per-entry sums
         unsigned long long* host_counters = nullptr;
         long long samples_done = 0;
         std::vector<unsigned char> dev_scene;  // packed DevScene<N>
@@ -1311,6 +1312,7 @@ struct PassJob
         long long total = 0;
         long long spp_eff = 0;
         bool smooth = false;
+        bool counts_samples = true;  // the pass adds to the scene's accumulator (its sample count grows)
         KernelTimes times;
         std::chrono::steady_clock::time_point t0;
         virtual ~PassJob() = default;
@@ -1338,14 +1340,32 @@ struct PassJobN final : PassJob
         }
 };
 
-// moments_accum: per-path sums (pixel * spp_eff + sample, 3 doubles each, zeroed by the caller)
-// instead of the scene's per-pixel accumulator (nt_render_moments).
-template <int N>
-std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, double* moments_accum)
+// Where a pass's radiance goes when it is not the scene's per-pixel accumulator.
+struct PassTarget
 {
+        double* moments = nullptr;        // per-path sums (pixel * spp_eff + sample, 3 doubles each, zeroed by
+                                          // the caller): nt_render_moments
+        const long long* list = nullptr;  // device pixel list: nt_render_pixels ...
+        long long list_count = 0;
+        double* list_accum = nullptr;     // ... and its per-entry sums (3 doubles each, zeroed by the caller)
+        long long first_sample = -1;      // >= 0: the pass's first sample index; < 0: from opts / the scene
+};
+
+// The first sample index of an ordinary pass: opts.sample_offset when positive, else the samples
+// already accumulated (progressive passes).
+long long pass_first_sample(const nt_scene* s, const nt_render_opts& o)
+{
+        return o.sample_offset > 0 ? (long long)o.sample_offset : s->samples_done;
+}
+
+template <int N>
+std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, const PassTarget& target = PassTarget())
+{
+        double* const moments_accum = target.moments;
         auto job = std::make_unique<PassJobN<N>>();
         job->t0 = std::chrono::steady_clock::now();
         job->s = s;
+        job->counts_samples = !target.moments && !target.list;
         if (o.samples_per_pixel < 1)
         {
                 fail(NT_EINVAL, "Stratified jittered sample count is not a positive integer");
@@ -1367,10 +1387,15 @@ std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, doub
         const bool smooth = smooth_shading(s, o);
         S.smooth_normal = smooth ? 1 : 0;
         const long long npix = s->pixel_count();
-        const long long total = npix * spp_eff;
-        if ((s->samples_done + spp_eff) * npix >= (1ll << 62) || s->samples_done + spp_eff > 0xffffffffll)
+        const long long first_sample = target.first_sample >= 0 ? target.first_sample : pass_first_sample(s, o);
+        const long long total = (target.list ? target.list_count : npix) * spp_eff;
+        if ((first_sample + spp_eff) * npix >= (1ll << 62) || first_sample + spp_eff > 0xffffffffll)
         {
                 fail(NT_EINVAL, "sample count overflow");
+        }
+        if (target.list && target.list_count > 0xffffffffll)
+        {
+                fail(NT_EINVAL, "too many pixels in one list");
         }
         const int lights = (int)s->lights.size();
         // default pool: 4 Mi paths (fewer wavefront iterations, so less per-launch tail), at most 1 GiB
@@ -1395,15 +1420,16 @@ std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, doub
         P.k1d = k;
         P.recip_k = 1.0f / k;
         P.npix = npix;
-        P.sample_offset = s->samples_done;
+        P.sample_offset = first_sample;
         P.path_begin = 0;
         P.path_end = total;
         P.moments = moments_accum ? 1 : 0;
+        P.list = target.list;
         if (moments_accum && total > 0xffffffffll)
         {
                 fail(NT_EINVAL, "too many paths in one moments pass");
         }
-        job->accum = moments_accum ? moments_accum : s->accum.as<double>();
+        job->accum = moments_accum ? moments_accum : (target.list ? target.list_accum : s->accum.as<double>());
         job->total = total;
         job->spp_eff = spp_eff;
         job->smooth = smooth;
@@ -1423,7 +1449,7 @@ void finish_pass(PassJob& job, const nt_render_opts& o, nt_stats* st, bool copy_
         }
         check_cuda(cudaStreamSynchronize(s->stream), "render sync");
         const bool stopped = (o.stop && *o.stop) || !s->host_counters[C_DONE];
-        s->samples_done += stopped ? 0 : job.spp_eff;
+        s->samples_done += (stopped || !job.counts_samples) ? 0 : job.spp_eff;
         if (st)
         {
                 const KernelTimes& times = job.times;
@@ -1462,9 +1488,9 @@ void finish_pass(PassJob& job, const nt_render_opts& o, nt_stats* st, bool copy_
 }
 
 template <int N>
-void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* moments_accum = nullptr)
+void render(nt_scene* s, const nt_render_opts& o, nt_stats* st, const PassTarget& target = PassTarget())
 {
-        std::unique_ptr<PassJob> job = prepare_pass<N>(s, o, moments_accum);
+        std::unique_ptr<PassJob> job = prepare_pass<N>(s, o, target);
         check_cuda(job->run(o), "render");
         finish_pass(*job, o, st, true);
 }
@@ -1545,7 +1571,7 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
         check_cuda(cudaMemsetAsync(counters, 0, C_COUNT * sizeof(unsigned long long), st), "memset counters");
         unsigned long long host_counters[C_COUNT] = {};
         KernelTimes times;
-        // enqueued directly: a graph instantiation may allocate, and the caller's stream may be capturing
+        // the iterations are enqueued directly, not through a CUDA graph: instantiating a graph may allocate
         check_cuda(W.run(S, P, d_accum, counters, host_counters, total, st, &times, false, o.stop, false), "render");
         check_cuda(cudaMemcpyAsync(host_counters, counters, C_COUNT * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st),
                    "counters");
@@ -1570,6 +1596,7 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
                 out->shadow_box_steps = (int64_t)host_counters[C_SH_BOX_STEPS];
                 out->shadow_retests = (int64_t)host_counters[C_SH_RETESTS];
                 out->shadow_descent_levels = (int64_t)host_counters[C_SH_DESCENT];
+                out->iterations = (int64_t)host_counters[C_ITERS];
                 out->seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         }
         if (stopped)
@@ -1643,15 +1670,15 @@ struct PrepareF
 {
         static void run(nt_scene* s, const nt_render_opts& o, std::unique_ptr<PassJob>* out)
         {
-                *out = prepare_pass<N>(s, o, nullptr);
+                *out = prepare_pass<N>(s, o);
         }
 };
 template <int N>
-struct MomentsF
+struct TargetF
 {
-        static void run(nt_scene* s, const nt_render_opts& o, nt_stats* st, double* acc)
+        static void run(nt_scene* s, const nt_render_opts& o, nt_stats* st, const PassTarget* target)
         {
-                render<N>(s, o, st, acc);
+                render<N>(s, o, st, *target);
         }
 };
 template <int N>
@@ -2268,6 +2295,61 @@ int nt_render(nt_scene* scene, const nt_render_opts* opts, nt_stats* stats)
         });
 }
 
+int nt_render_pixels(nt_scene* scene, const nt_render_opts* opts, const int64_t* pixels, int64_t count,
+                     float* rgb_mean, nt_stats* stats)
+{
+        return guarded([&]() {
+                need_built(scene);
+                if (!opts || !pixels || !rgb_mean || count < 1)
+                {
+                        fail(NT_EINVAL, "bad pixel-list arguments");
+                }
+                const long long npix = scene->pixel_count();
+                for (int64_t i = 0; i < count; ++i)
+                {
+                        if (pixels[i] < 0 || pixels[i] >= npix)
+                        {
+                                fail(NT_EINVAL, "pixel index " + std::to_string(pixels[i]) + " out of range");
+                        }
+                }
+                const int spp = nt_effective_spp(scene->n, opts->samples_per_pixel);
+                if (spp < 1)
+                {
+                        fail(NT_EINVAL, "Stratified jittered sample count is not a positive integer");
+                }
+                const size_t list_bytes = (size_t)count * sizeof(long long);
+                const size_t sum_bytes = (size_t)count * 3 * sizeof(double);
+                if (scene->list_buf.bytes < list_bytes + sum_bytes)
+                {
+                        scene->list_buf.alloc(list_bytes + sum_bytes);
+                }
+                if (scene->mean_buf.bytes < (size_t)count * 3 * sizeof(float))
+                {
+                        scene->mean_buf.alloc((size_t)count * 3 * sizeof(float));
+                }
+                long long* d_list = scene->list_buf.as<long long>();
+                double* d_sums = reinterpret_cast<double*>(scene->list_buf.as<char>() + list_bytes);
+                check_cuda(cudaMemcpyAsync(d_list, pixels, list_bytes, cudaMemcpyHostToDevice, scene->stream), "copy pixels");
+                check_cuda(cudaMemsetAsync(d_sums, 0, sum_bytes, scene->stream), "memset");
+                PassTarget target;
+                target.list = d_list;
+                target.list_count = count;
+                target.list_accum = d_sums;
+                target.first_sample = std::max<long long>(opts->sample_offset, 0);
+                nt_stats one{};
+                dispatch<TargetF>(scene->n, scene, *opts, &one, &target);
+                check_cuda(launch_mean(count * 3, d_sums, spp, scene->mean_buf.as<float>(), scene->stream), "mean");
+                check_cuda(cudaMemcpyAsync(rgb_mean, scene->mean_buf.p, (size_t)count * 3 * sizeof(float),
+                                           cudaMemcpyDeviceToHost, scene->stream),
+                           "copy mean");
+                check_cuda(cudaStreamSynchronize(scene->stream), "sync");
+                if (stats)
+                {
+                        *stats = one;
+                }
+        });
+}
+
 int nt_render_aux(nt_scene* scene, float* d_normal, float* d_depth, void* stream)
 {
         return guarded([&]() {
@@ -2303,9 +2385,11 @@ int nt_render_moments(nt_scene* scene, const nt_render_opts* opts, int64_t sampl
                         scene->moments.alloc(bytes);
                 }
                 check_cuda(cudaMemsetAsync(scene->moments.p, 0, bytes, scene->stream), "memset");
-                scene->samples_done = sample_offset;
+                PassTarget target;
+                target.moments = scene->moments.as<double>();
+                target.first_sample = sample_offset;
                 nt_stats one{};
-                dispatch<MomentsF>(scene->n, scene, *opts, &one, scene->moments.as<double>());
+                dispatch<TargetF>(scene->n, scene, *opts, &one, &target);
                 check_cuda(launch_moments_reduce(npix, spp, scene->moments.as<double>(), d_mean, d_var, scene->stream),
                            "moments");
                 check_cuda(cudaStreamSynchronize(scene->stream), "moments sync");

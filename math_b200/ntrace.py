@@ -37,10 +37,10 @@ EXPORTED_SYMBOLS = (
     "nt_scene_object_count", "nt_accum_read_srgb_slice", "nt_convex_hull", "nt_hull_facet_count", "nt_hull_facets",
     "nt_hull_destroy", "nt_scene_clear_lights", "nt_render_batch",
     "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
-    "nt_render_moments", "nt_render_noalloc",
+    "nt_render_moments", "nt_render_noalloc", "nt_render_pixels",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
     "nt_denoiser_set_params", "nt_denoiser_set_input", "nt_denoiser_apply", "nt_denoiser_gradient",
-    "nt_denoiser_train_step", "nt_tc_gemm_bf16",
+    "nt_denoiser_train_step", "nt_tc_gemm_bf16", "nt_tc_gemm_wait_selftest",
 )
 
 
@@ -62,7 +62,8 @@ class BuildOpts(ctypes.Structure):
 class RenderOpts(ctypes.Structure):
     _fields_ = [("samples_per_pixel", ctypes.c_int), ("max_depth", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("retest", ctypes.c_int), ("smooth_normal", ctypes.c_int), ("pool_paths", ctypes.c_int64),
-                ("timing", ctypes.c_int), ("stop", ctypes.c_void_p), ("graph_iterations", ctypes.c_int)]
+                ("timing", ctypes.c_int), ("stop", ctypes.c_void_p), ("graph_iterations", ctypes.c_int),
+                ("sample_offset", ctypes.c_int64)]
 
 
 class Stats(ctypes.Structure):
@@ -153,6 +154,7 @@ def library() -> ctypes.CDLL:
         "nt_scene_set_object_surface": ([vp, ctypes.c_int, ctypes.POINTER(Surface)], ctypes.c_int),
         "nt_render_aux": ([vp, vp, vp, vp], ctypes.c_int),
         "nt_render_moments": ([vp, ctypes.POINTER(RenderOpts), i64, vp, vp, ctypes.POINTER(Stats)], ctypes.c_int),
+        "nt_render_pixels": ([vp, ctypes.POINTER(RenderOpts), vp, i64, vp, ctypes.POINTER(Stats)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)
@@ -210,9 +212,10 @@ def cosine_sphere_coefficient(n: int) -> float:
 
 def render_opts(samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                 smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False,
-                graph_iterations: int = 0) -> RenderOpts:
+                graph_iterations: int = 0, sample_offset: int = 0) -> RenderOpts:
     return RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)),
-                      int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None, int(graph_iterations))
+                      int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None, int(graph_iterations),
+                      int(sample_offset))
 
 
 def render_batch(scenes: list, opts: list[dict]) -> list[dict]:
@@ -352,14 +355,34 @@ class Scene:
 
     def render(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None,
-               graph_iterations: int = 0) -> dict:
+               graph_iterations: int = 0, sample_offset: int = 0) -> dict:
+        """One pass added to the accumulator (nt_render); sample_offset > 0 starts it at that sample
+        index, 0 continues after the accumulated samples."""
         o = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, pool_paths, timing,
-                        graph_iterations)
+                        graph_iterations, sample_offset)
         if stop is not None:
             o.stop = ctypes.cast(stop, ctypes.c_void_p)
         st = Stats()
         _check(self._lib.nt_render(self._h, ctypes.byref(o), ctypes.byref(st)))
         return st.as_dict()
+
+    def render_pixels(self, pixels, samples_per_pixel: int, max_depth: int = 100, seed: int = 0,
+                      retest: bool = True, smooth_normal: bool = False, pool_paths: int = 0,
+                      sample_offset: int = 0) -> tuple[np.ndarray, dict]:
+        """Mean colour of each listed pixel over samples [sample_offset, + effective spp)
+        (nt_render_pixels).  pixels: linear indices, or an (m, n-1) array of screen coordinates."""
+        px = np.asarray(pixels)
+        if px.ndim == 2:
+            strides = np.cumprod([1] + list(self.screen[:-1]), dtype=np.int64)
+            px = (px.astype(np.int64) * strides).sum(axis=1)
+        lin = np.ascontiguousarray(px, dtype=np.int64).reshape(-1)
+        out = np.zeros((len(lin), 3), np.float32)
+        o = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, pool_paths, False, 0,
+                        sample_offset)
+        st = Stats()
+        _check(self._lib.nt_render_pixels(self._h, ctypes.byref(o), lin.ctypes.data, len(lin), out.ctypes.data,
+                                          ctypes.byref(st)))
+        return out, st.as_dict()
 
     def autotune(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                  smooth_normal: bool = False) -> tuple[dict, float]:
