@@ -77,6 +77,13 @@ int nt_denoiser_train_step(nt_denoiser* d, const float* d_target, float lr, doub
  * N <= 256.  stream: a cudaStream_t or NULL (the default stream). */
 int nt_tc_gemm_bf16(const uint16_t* d_a, const uint16_t* d_b, float* d_c, int m, int n, int k, void* stream);
 
+/* Failure-detection self-test of the GEMM kernel: one small launch with its tensor-core instructions
+ * withheld, so that the kernel's bounded wait for their completion (20 ms here, about a second in
+ * ordinary launches) runs out; the kernel then gives its tensor memory back, raises its error flag and
+ * returns.  Returns NT_ETIMEOUT when that happened as designed (the CUDA context stays usable), NT_OK if
+ * the wait did not run out (a broken self-test), or another code on a CUDA error. */
+int nt_tc_gemm_wait_selftest(void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,14 @@ __host__ __device__ constexpr uint32_t umma_idesc_bf16(int m, int n)
         return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
+// Bounds of the GEMM's completion waits.  withhold = 1 is the failure-detection self-test: the MMAs
+// and their commit are not issued, so nothing ever arrives on the barrier and every wait runs out.
+struct GemmCtl
+{
+        unsigned long long wait_ns = 1000000000ull;  // about a second
+        int withhold = 0;
+};
+
 __device__ __forceinline__ unsigned long long global_ns()
 {
         unsigned long long t;
@@ -82,8 +90,8 @@ __device__ __forceinline__ unsigned long long global_ns()
         return t;
 }
 
-// Waits for the mbarrier phase `parity` to complete; gives up after about a second.
-__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity)
+// Waits for the mbarrier phase `parity` to complete; gives up after limit_ns nanoseconds.
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t parity, unsigned long long limit_ns)
 {
         const uint32_t addr = smem_u32(bar);
         const unsigned long long t0 = global_ns();
@@ -101,7 +109,7 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t pari
                 {
                         return true;
                 }
-                if (global_ns() - t0 > 1000000000ull)
+                if (global_ns() - t0 > limit_ns)
                 {
                         return false;
                 }
@@ -131,7 +139,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
 // at most 256; ncols: tensor-memory columns (power of two >= max(32, N)).
 template <class LA, class LB, class EPI>
 __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, const EPI epi, int M, int N, int K,
-                                                   int k_per_cta, uint32_t ncols, int* err)
+                                                   int k_per_cta, uint32_t ncols, int* err, const GemmCtl ctl)
 {
         extern __shared__ __align__(1024) unsigned char g_smem[];
         __shared__ __align__(8) unsigned long long s_bar;
@@ -239,7 +247,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
                 // the tensor core reads shared memory through the async proxy
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncthreads();
-                if (tid == 0)
+                if (tid == 0 && !ctl.withhold)
                 {
                         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 #pragma unroll
@@ -261,7 +269,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
                 }
                 pending = true;
                 // the stage is overwritten next: wait until the MMAs have read it
-                const bool done = mbar_wait(&s_bar, parity);
+                const bool done = mbar_wait(&s_bar, parity, ctl.wait_ns);
                 ok = __syncthreads_and(done) != 0;
                 if (!ok)
                 {
@@ -275,7 +283,7 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
         {
                 // a commit that did not arrive in time: wait once more (bounded) before the
                 // accumulator's columns are given back
-                mbar_wait(&s_bar, parity);
+                mbar_wait(&s_bar, parity, ctl.wait_ns);
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (ok && stages > 0)
@@ -521,7 +529,7 @@ uint32_t tmem_cols(int n)
 
 template <class LA, class LB, class EPI>
 cudaError_t gemm(const LA& la, const LB& lb, const EPI& epi, int M, int N, int K, int k_per_cta, int* err,
-                 cudaStream_t st)
+                 cudaStream_t st, const GemmCtl ctl = GemmCtl{})
 {
         if (M <= 0 || K <= 0)
         {
@@ -559,7 +567,7 @@ cudaError_t gemm(const LA& la, const LB& lb, const EPI& epi, int M, int N, int K
         }
         const int kpc = k_per_cta > 0 ? (k_per_cta + GK - 1) / GK * GK : (K + GK - 1) / GK * GK;
         dim3 grid((unsigned)((M + GM - 1) / GM), (unsigned)((K + kpc - 1) / kpc));
-        k_gemm<LA, LB, EPI><<<grid, GTHREADS, smem, st>>>(la, lb, epi, M, N, K, kpc, ncols, err);
+        k_gemm<LA, LB, EPI><<<grid, GTHREADS, smem, st>>>(la, lb, epi, M, N, K, kpc, ncols, err, ctl);
         return cudaGetLastError();
 }
 
@@ -1457,6 +1465,35 @@ int nt_denoiser_train_step(nt_denoiser* d, const float* d_target, float lr, doub
                 if (loss)
                 {
                         *loss = l;
+                }
+        });
+}
+
+int nt_tc_gemm_wait_selftest(void* stream)
+{
+        return guard([&]() {
+                cudaStream_t s = (cudaStream_t)stream;
+                Buf a, b, c, err;
+                const int m = 128, n = 16, k = 64;
+                a.ensure((size_t)m * k * 2);
+                b.ensure((size_t)n * k * 2);
+                c.ensure((size_t)m * n * 4);
+                err.ensure(sizeof(int));
+                ck(cudaMemsetAsync(a.p, 0, (size_t)m * k * 2, s), "memset");
+                ck(cudaMemsetAsync(b.p, 0, (size_t)n * k * 2, s), "memset");
+                ck(cudaMemsetAsync(err.p, 0, sizeof(int), s), "memset");
+                GemmCtl ctl;
+                ctl.wait_ns = 20000000ull;  // 20 ms
+                ctl.withhold = 1;
+                ck(gemm(LoadRows{a.as<const __nv_bfloat16>(), k}, LoadRows{b.as<const __nv_bfloat16>(), k}, EpiStoreF32{c.as<float>(), n},
+                        m, n, k, 0, err.as<int>(), s, ctl),
+                   "gemm");
+                int h = 0;
+                ck(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+                ck(cudaStreamSynchronize(s), "sync");
+                if (h)
+                {
+                        throw DError{NT_ETIMEOUT, "tensor-core GEMM: an MMA completion wait ran out"};
                 }
         });
 }

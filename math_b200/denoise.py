@@ -50,6 +50,7 @@ def _lib() -> ctypes.CDLL:
             "nt_denoiser_gradient": ([vp, vp, vp, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "nt_denoiser_train_step": ([vp, vp, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "nt_tc_gemm_bf16": ([vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
+            "nt_tc_gemm_wait_selftest": ([vp], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)
@@ -83,6 +84,14 @@ def tc_gemm(a, b):
     _check(_lib().nt_tc_gemm_bf16(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, n, k,
                                   torch.cuda.current_stream().cuda_stream or None))
     return c
+
+
+def tc_gemm_wait_selftest() -> int:
+    """Runs the GEMM kernel's failure-detection self-test (its completion wait made to run out);
+    returns the NT_* status (NT_ETIMEOUT when the kernel detected and reported the timeout)."""
+    import torch
+
+    return int(_lib().nt_tc_gemm_wait_selftest(torch.cuda.current_stream().cuda_stream or None))
 
 
 class Denoiser:

@@ -182,6 +182,25 @@ def test_tc_gemm_matches_torch(require_gpu, m, n, k):
     assert err <= 1e-3 * max(1.0, ref.abs().max().item()), err
 
 
+@pytest.mark.gpu
+def test_tc_gemm_wait_runs_out_and_reports(require_gpu):
+    """Failure detection without a fault: the GEMM kernel with its tensor-core instructions withheld
+    (nothing ever arrives on its barrier) gives up its bounded wait, frees its tensor memory and reports
+    NT_ETIMEOUT; the context stays usable (an ordinary GEMM right after is correct)."""
+    torch = _torch()
+    from math_b200 import ntrace
+    from math_b200.denoise import tc_gemm, tc_gemm_wait_selftest
+
+    assert tc_gemm_wait_selftest() == ntrace.NT_ETIMEOUT
+    assert b"completion wait ran out" in ntrace.library().nt_last_error_message()
+    g = torch.Generator(device="cpu").manual_seed(5)
+    a = torch.randn(256, 64, generator=g).to(torch.bfloat16).cuda()
+    b = torch.randn(32, 64, generator=g).to(torch.bfloat16).cuda()
+    c = tc_gemm(a, b)
+    ref = a.float() @ b.float().T
+    assert (c - ref).abs().max().item() <= 1e-3 * ref.abs().max().item()
+
+
 def _gpu_inputs(n, screen, seed):
     torch = _torch()
     mean, var, normal, depth, target = _random_inputs(n, screen, np.random.default_rng(seed))
