@@ -115,29 +115,32 @@ def algorithmic_work(n: int, facet_tests: int, box_steps: int, descent: int) -> 
     return b, f
 
 
+def pixel_sample(screen, count: int, rng) -> np.ndarray:
+    """`count` distinct random pixels of the screen as (count, n-1) coordinates."""
+    npix = int(np.prod(screen))
+    lin = np.sort(rng.choice(npix, count, replace=False))
+    return np.stack([(lin // int(np.prod(screen[:j]))) % screen[j] for j in range(len(screen))], axis=1)
+
+
 def cpu_baseline(spec: dict, paths_target: int, threads: int) -> dict:
-    """The reference painter on the host cores over a seeded random pixel sample of the frame."""
+    """The reference painter (its own -Ofast build) on the host cores over a seeded random pixel
+    sample of the frame."""
+    from math_b200 import scenes
     from oracle import checkers
 
     n = spec["n"]
     screen = spec["projector"]["screen"]
     npix = int(np.prod(screen))
-    spp_eff = checkers.Port().effective_spp(n, spec["spp"])
+    spp_eff = scenes.effective_spp(n, spec["spp"])
     count = int(min(npix, max(1000, paths_target // spp_eff)))
-    rng = np.random.default_rng(12345)
-    lin = np.sort(rng.choice(npix, count, replace=False))
-    px = np.empty((count, n - 1), np.int64)
-    rem = lin.copy()
-    for j in range(n - 1):
-        px[:, j] = rem % screen[j]
-        rem //= screen[j]
-    if checkers.Reference.available():
-        ref = checkers.Reference()
+    px = pixel_sample(screen, count, np.random.default_rng(12345))
+    if checkers.Reference.available(fast=True):
+        ref = checkers.Reference(fast=True)
         _, st = ref.paint(spec, dbl=False, seed=1, threads=threads, pixels=px, store=False)
         return {"value": st["sample_count"] / st["seconds"], "unit": "paths/s", "cores": threads,
-                "kind": "reference", "seconds": st["seconds"],
+                "kind": "reference", "seconds": st["seconds"], "build": ref.flags,
                 "sample": f"{count} random pixels of the {'x'.join(map(str, screen))} frame x {spp_eff} spp "
-                          f"= {st['sample_count']} paths, paint<{n},float>() with {threads} threads"}
+                          f"= {st['sample_count']} paths, paint<{n},float>() ({ref.flags}) with {threads} threads"}
     port = checkers.Port()
     _, st = port.paint(spec, dbl=False, threads=threads, pixels=px)
     return {"value": st["paths"] / st["seconds"], "unit": "paths/s", "cores": threads, "kind": "port",
@@ -146,53 +149,70 @@ def cpu_baseline(spec: dict, paths_target: int, threads: int) -> dict:
 
 
 def run_reference(args) -> None:
+    """The reference painter alone in this process: the scene's mesh comes from scipy's Qhull (the
+    same facet set as the library's hull) and the sample sizes from a Python restatement, so that
+    nothing of math_b200's native code is loaded; the painter is the reference's own -Ofast build."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     from math_b200 import scenes
     from oracle import checkers
 
-    spec = scenes.config(args.config)
+    if not checkers.Reference.available(fast=True):
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/fast/libref_painter.so is not built"}))
+        return
+    spec = scenes.config(args.config, hull="qhull")
     threads = os.cpu_count() or 1
     n = spec["n"]
-    if not checkers.Reference.available():
-        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libref_painter.so is not built"}))
-        return
-    ref = checkers.Reference()
+    ref = checkers.Reference(fast=True)
     screen = spec["projector"]["screen"]
     npix = int(np.prod(screen))
-    spp_eff = checkers.Port().effective_spp(n, spec["spp"])
+    spp_eff = scenes.effective_spp(n, spec["spp"])
     count = min(npix, args.cpu_paths // spp_eff)
     rng = np.random.default_rng(7)
     total_paths, total_s = 0, 0.0
     for step in range(args.warmup + args.steps):
-        lin = np.sort(rng.choice(npix, count, replace=False))
-        px = np.stack([(lin // int(np.prod(screen[:j]))) % screen[j] for j in range(n - 1)], axis=1)
+        px = pixel_sample(screen, count, rng)
         _, st = ref.paint(spec, dbl=False, seed=step + 1, threads=threads, pixels=px, store=False)
         if step >= args.warmup:
             total_paths += st["sample_count"]
             total_s += st["seconds"]
     value = total_paths / total_s
     sample = (f"per step {count} random pixels of the {'x'.join(map(str, screen))} frame x {spp_eff} spp, "
-              f"paint<{n},float>() of the reference with {threads} threads")
+              f"paint<{n},float>() of the reference ({ref.flags}) with {threads} threads; mesh: the same "
+              f"facet set from scipy's Qhull")
     print(json.dumps({
         "impl": "reference", "metric": metric_name(spec["n"]), "value": value, "unit": "paths/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * total_s / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_block(spec, args),
+        "mesh": mesh_block(spec, "scipy Qhull of the same points (the library's exact hull differs in the "
+                                 "triangulation of a few near-degenerate regions)"),
         "cpu_baseline": {"value": value, "unit": "paths/s", "cores": threads, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "paths/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
 
 
+WORKLOAD_MESH = {
+    "n3": "icosphere subdivided 5 times (20,480 triangles)",
+    "n4": "hull boundary of 100,000 seeded points on S^3 (tetrahedra)",
+    "n5": "hull boundary of 50,000 seeded points on S^4 without a cap of angular radius 0.5 (4-simplices)",
+}
+
+
 def config_block(spec: dict, args) -> dict:
+    """The workload, identical in both arms (what differs between them goes in mesh_block)."""
     n = spec["n"]
-    return {"workload": f"n={n} plain tracer: {len(spec['facets'])}-facet sphere hull mesh + floor + point light, "
+    return {"workload": f"n={n} plain tracer: {WORKLOAD_MESH[args.config]} + floor + point light, "
                         f"parallel projection {'x'.join(map(str, spec['projector']['screen']))}, "
                         f"{spec['spp']} spp, depth {spec['max_depth']}, FP32 + FP64 re-test",
-            "n": n, "facets": int(len(spec["facets"])), "screen": spec["projector"]["screen"], "spp": spec["spp"],
+            "n": n, "screen": spec["projector"]["screen"], "spp": spec["spp"],
             "max_depth": spec["max_depth"], "seed": spec["seed"],
             "l2": "scene arrays larger than the 126 MB L2; no flush between steps"}
+
+
+def mesh_block(spec: dict, hull: str) -> dict:
+    return {"facets": int(len(spec["facets"])), "vertices": int(len(spec["verts"])), "hull": hull}
 
 
 def main() -> None:
@@ -236,8 +256,17 @@ def main() -> None:
 
     # the library's autotuner picks the path-pool size and the iterations per graph launch from probe
     # passes of this frame (untimed; it clears the accumulator)
-    tuned, _ = scene.autotune(spp, max_depth=depth, seed=spec["seed"] + rank)
-    ropts = dict(max_depth=depth, seed=spec["seed"] + rank, pool_paths=tuned["pool_paths"],
+    tuned, _ = scene.autotune(spp, max_depth=depth, seed=spec["seed"])
+    # every rank traces the same Philox stream; ranks take disjoint sample ranges (pass k of rank r
+    # covers samples [(k * world + r) * spp_eff, + spp_eff)), so N ranks render N different passes
+    from math_b200 import distributed
+
+    spp_eff = scenes.effective_spp(n, spp)
+
+    def offset(k: int) -> int:
+        return distributed.sample_offset(rank, k, spp_eff, world)
+
+    ropts = dict(max_depth=depth, seed=spec["seed"], pool_paths=tuned["pool_paths"],
                  graph_iterations=tuned["graph_iterations"])
 
     # warm-up (also the per-kernel timing pass: device events around every launch)
@@ -255,8 +284,8 @@ def main() -> None:
             dist.barrier()
         torch.cuda.synchronize()
         ev0.record(stream)
-        for _ in range(args.steps):
-            stats.append(scene.render(spp, **ropts))
+        for k in range(args.steps):
+            stats.append(scene.render(spp, **ropts, sample_offset=offset(k)))
         ev1.record(stream)
         torch.cuda.synchronize()
         if dist:
@@ -273,7 +302,7 @@ def main() -> None:
     ms_max = float(ms_all.item())
     value = float(paths_all.item()) / (ms_max / 1000.0)
 
-    # combine the ranks' samples (independent Philox keys per rank) into one image: one NCCL
+    # combine the ranks' samples (disjoint sample ranges of one Philox stream) into one image: one NCCL
     # all-reduce of the per-pixel sums, after the timed region
     combine_ms = None
     if dist:
@@ -301,7 +330,7 @@ def main() -> None:
         scene.upload_commit()
         if k + 1 < e2e_steps:
             scene.upload_begin()
-        st = scene.render(spp, **ropts)
+        st = scene.render(spp, **ropts, sample_offset=offset(k))
         scene.image(out=host_img)
         e2e_paths += st["paths"]
         d2h = host_img.nbytes
@@ -342,8 +371,10 @@ def main() -> None:
         "metric": metric_name(n), "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": dict(config_block(spec, args), pool_paths=tuned["pool_paths"],
-                       graph_iterations=tuned["graph_iterations"], tuned_by="nt_autotune"),
+        "config": config_block(spec, args),
+        "mesh": mesh_block(spec, "exact (nt_convex_hull)"),
+        "tuning": {"pool_paths": tuned["pool_paths"], "graph_iterations": tuned["graph_iterations"],
+                   "tuned_by": "nt_autotune"},
         "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "steps": e2e_steps},
         "gpu_launches": launches,

@@ -20,14 +20,23 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 PORT_LIB = HERE / "_lib" / "libntrace_oracle.so"
 REF_LIB = HERE / "_ref" / "libref_painter.so"
-REFERENCE_ROOT = Path(os.environ.get("NTRACE_REFERENCE_ROOT", "/root/reference"))
+REF_FAST_LIB = HERE / "_ref" / "fast" / "libref_painter.so"
+
+
+def reference_root() -> Path:
+    """The reference checkout: $NTRACE_REFERENCE_ROOT, else the directory "reference" beside this
+    checkout (in the same parent directory)."""
+    env = os.environ.get("NTRACE_REFERENCE_ROOT")
+    return Path(env) if env else HERE.parents[1] / "reference"
 
 
 def build(ref: bool = True) -> None:
-    """Builds the port, and the reference bridge when the reference sources are present."""
+    """Builds the port, and both reference builds (parity: -O2 without contraction; timing: the
+    reference's own -Ofast) when the reference sources are present."""
     subprocess.run(["make", "-s", "-C", str(HERE), "port"], check=True)
-    if ref and (REFERENCE_ROOT / "src" / "painter" / "painter.cpp").exists():
-        subprocess.run(["make", "-s", "-C", str(HERE), "ref", f"REF_ROOT={REFERENCE_ROOT}"], check=True)
+    root = reference_root()
+    if ref and (root / "src" / "painter" / "painter.cpp").exists():
+        subprocess.run(["make", "-s", "-C", str(HERE), "ref", "ref_fast", f"REF_ROOT={root}"], check=True)
 
 
 class SceneStruct(ctypes.Structure):
@@ -46,6 +55,10 @@ class SceneStruct(ctypes.Structure):
         ("bg_color", ctypes.c_float * 3), ("bg_light_color", ctypes.c_float * 3), ("bg_is_light", ctypes.c_int),
         ("smooth_normal", ctypes.c_int), ("tree_threads", ctypes.c_int),
         ("normals", ctypes.c_void_p), ("nnormals", ctypes.c_long), ("facet_normals", ctypes.c_void_p),
+        ("verts2", ctypes.c_void_p), ("nverts2", ctypes.c_long), ("facets2", ctypes.c_void_p), ("nfacets2", ctypes.c_long),
+        ("mesh2_color", ctypes.c_float * 3), ("mesh2_diffuse", ctypes.c_float),
+        ("has_hplt", ctypes.c_int), ("hplt_org", ctypes.c_float * 6), ("hplt_edges", ctypes.c_float * 30),
+        ("hplt_color", ctypes.c_float * 3), ("hplt_diffuse", ctypes.c_float),
     ]
 
 
@@ -125,6 +138,27 @@ def scene_struct(spec: dict, dbl: bool, threads: int = 1) -> tuple[SceneStruct, 
             fn = np.ascontiguousarray(spec["facet_normals"], dtype=np.int32).reshape(-1, n)
             keep.append(fn)
             s.facet_normals = fn.ctypes.data
+    m2 = spec.get("mesh2")
+    if m2 is not None:
+        v = np.ascontiguousarray(m2["verts"], dtype=np.float32).reshape(-1, n)
+        f = np.ascontiguousarray(m2["facets"], dtype=np.int32).reshape(-1, n)
+        keep += [v, f]
+        s.verts2, s.nverts2, s.facets2, s.nfacets2 = v.ctypes.data, len(v), f.ctypes.data, len(f)
+        for i in range(3):
+            s.mesh2_color[i] = m2["color"][i]
+        s.mesh2_diffuse = m2["diffuse"]
+    hp = spec.get("hplt")
+    if hp is not None:
+        s.has_hplt = 1
+        e = np.asarray(hp["edges"], np.float32).reshape(n - 1, n)
+        for k in range(n):
+            s.hplt_org[k] = hp["org"][k]
+        for i in range(n - 1):
+            for k in range(n):
+                s.hplt_edges[i * n + k] = e[i, k]
+        for i in range(3):
+            s.hplt_color[i] = hp["color"][i]
+        s.hplt_diffuse = hp["diffuse"]
     return s, keep
 
 
@@ -250,13 +284,18 @@ class Reference:
     """The reference painter compiled from its own sources (available where it was built)."""
 
     @staticmethod
-    def available() -> bool:
-        return REF_LIB.exists()
+    def available(fast: bool = False) -> bool:
+        return (REF_FAST_LIB if fast else REF_LIB).exists()
 
-    def __init__(self):
-        if not REF_LIB.exists():
-            raise FileNotFoundError(f"{REF_LIB} is not built (the reference sources are needed to build it)")
-        lib = ctypes.CDLL(str(REF_LIB))
+    def __init__(self, fast: bool = False):
+        """fast=False: the parity build (IEEE order); fast=True: the reference's own -Ofast -mavx -mfma
+        build, for timing."""
+        path = REF_FAST_LIB if fast else REF_LIB
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is not built (the reference sources are needed to build it)")
+        self.path = path
+        self.flags = "-Ofast -mavx -mfma" if fast else "-O2 -mavx -mfma -ffp-contract=off"
+        lib = ctypes.CDLL(str(path))
         vp = ctypes.c_void_p
         lib.refb_mesh_create.restype = vp
         lib.refb_mesh_create.argtypes = [ctypes.c_int, ctypes.c_int, vp, ctypes.c_long, vp, ctypes.c_long, ctypes.c_int,
