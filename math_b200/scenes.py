@@ -10,11 +10,13 @@ Meshes:
   * ``sphere_hull(n, count, seed, cap)``: the boundary of the convex hull of ``count`` seeded points
     uniform on the unit (n-1)-sphere (normalised Gaussian vectors, numpy PCG64 seeded with ``seed``),
     optionally without the facets whose centroid lies within angular radius ``cap`` of +x_(n-1).  The
-    hull is computed with Qhull (scipy.spatial.ConvexHull) on the float32 points, so every facet
-    references exactly the vertices the tracer uses.
+    hull is the library's exact convex hull (``nt_convex_hull``) of the float32 points, so every facet
+    references exactly the vertices the tracer uses; ``method="qhull"`` takes scipy's Qhull instead,
+    which gives the same facet set in another order (for processes that must not load the library).
 
 A scene is a plain dict (``spec``) so that the same description feeds the product
-(:func:`build_scene`) and the checkers in ``oracle/``.
+(:func:`build_scene`) and the checkers in ``oracle/``.  Objects are added in the order mesh, second
+mesh (``spec["mesh2"]``), floor parallelotope, hyperplane parallelotope (``spec["hplt"]``).
 """
 
 from __future__ import annotations
@@ -30,6 +32,8 @@ from . import ntrace
 BACKGROUND = (0.30, 0.35, 0.40)
 BACKGROUND_LIGHT = (0.343, 0.343, 0.343)
 ALBEDO = 0.7
+# projector kinds (NT_PROJECTOR_*, include/ntrace.h)
+PARALLEL, PERSPECTIVE, SPHERICAL = 0, 1, 2
 
 
 def icosphere(subdivisions: int) -> tuple[np.ndarray, np.ndarray]:
@@ -100,7 +104,7 @@ def floor_slab(n: int) -> tuple[np.ndarray, np.ndarray]:
 
 def make_spec(n: int, verts: np.ndarray | None, facets: np.ndarray | None, screen: int, spp: int, max_depth: int = 5,
               seed: int = 0, floor: bool = True, extent: float = 8.0, light_kind: int = 0,
-              projector: int = ntrace.PARALLEL) -> dict:
+              projector: int = 0) -> dict:
     """A floor scene: mesh, floor slab, one light at (2, ..., 2, 3), parallel projection of
     [-extent/2, extent/2]^(n-1) seen from +x_(n-1)."""
     light = np.full(n, 2.0, np.float32)
@@ -120,7 +124,7 @@ def make_spec(n: int, verts: np.ndarray | None, facets: np.ndarray | None, scree
         "light": {"kind": light_kind, "pos": light, "color": (1.0, 1.0, 1.0),
                   "unit": float(np.linalg.norm(light.astype(np.float64)))},
         "projector": {"kind": projector, "org": cam, "dir": cdir, "axes": axes,
-                      "param": extent / screen if projector == ntrace.PARALLEL else 60.0,
+                      "param": extent / screen if projector == PARALLEL else 60.0,
                       "screen": [screen] * (n - 1)},
         "bg": {"color": BACKGROUND, "light": True, "light_color": BACKGROUND_LIGHT},
         "spp": spp,
@@ -133,30 +137,87 @@ def make_spec(n: int, verts: np.ndarray | None, facets: np.ndarray | None, scree
     return spec
 
 
-def config(name: str) -> dict:
-    """The measured configurations (full size) and their reduced test-size counterparts."""
+def config(name: str, hull: str = "ntrace") -> dict:
+    """The measured configurations (full size) and their reduced test-size counterparts.  hull: the
+    convex-hull method of the sphere meshes (see sphere_hull; "qhull" keeps the library unloaded)."""
     if name == "n3":
         v, f = icosphere(5)
         return make_spec(3, v, f, screen=400, spp=16)
     if name == "n4":
-        v, f = sphere_hull(4, 100_000, seed=0)
+        v, f = sphere_hull(4, 100_000, seed=0, method=hull)
         return make_spec(4, v, f, screen=128, spp=16)
     if name == "n5":
-        v, f = sphere_hull(5, 50_000, seed=0, cap=0.5)
+        v, f = sphere_hull(5, 50_000, seed=0, cap=0.5, method=hull)
         return make_spec(5, v, f, screen=48, spp=4)
+    if name == "n6":
+        v, f = sphere_hull(6, 400, seed=0, method=hull)
+        return make_spec(6, v, f, screen=12, spp=4)
     if name == "n3_small":
         v, f = icosphere(2)
         return make_spec(3, v, f, screen=48, spp=16)
     if name == "n4_small":
-        v, f = sphere_hull(4, 800, seed=1)
+        v, f = sphere_hull(4, 800, seed=1, method=hull)
         return make_spec(4, v, f, screen=12, spp=8)
     if name == "n5_small":
-        v, f = sphere_hull(5, 300, seed=2, cap=0.5)
+        v, f = sphere_hull(5, 300, seed=2, cap=0.5, method=hull)
         return make_spec(5, v, f, screen=6, spp=4)
     if name == "n6_small":
-        v, f = sphere_hull(6, 120, seed=3)
+        v, f = sphere_hull(6, 120, seed=3, method=hull)
         return make_spec(6, v, f, screen=4, spp=2)
     raise KeyError(name)
+
+
+INTERFACE_SCENES = ("constant_light_n4", "perspective_n4", "spherical_n5", "hplt_n4", "two_mesh_n3")
+
+
+def interface_scene(name: str) -> dict:
+    """Small scenes that use the scene types the measured configurations do not: a ConstantLight, the
+    perspective and spherical projectors, a hyperplane parallelotope, and two meshes (a closed sphere
+    and an open bowl standing on the floor, whose rays start inside the bowl's root box: the sorted
+    early break of ray_intersection with the root box's exit distance, ray_intersection.h:26-105)."""
+    if name == "constant_light_n4":
+        v, f = sphere_hull(4, 800, seed=1)
+        spec = make_spec(4, v, f, screen=12, spp=8, light_kind=1)
+        spec["light"]["color"] = (0.6, 0.5, 0.4)
+        return spec
+    if name == "perspective_n4":
+        v, f = sphere_hull(4, 800, seed=1)
+        spec = make_spec(4, v, f, screen=12, spp=8, projector=PERSPECTIVE)
+        spec["projector"]["org"] = np.array([0.3, -0.2, 0.1, 3.5], np.float32)
+        spec["projector"]["param"] = 70.0
+        return spec
+    if name == "spherical_n5":
+        v, f = sphere_hull(5, 300, seed=2, cap=0.5)
+        spec = make_spec(5, v, f, screen=6, spp=4, projector=SPHERICAL)
+        spec["projector"]["org"] = np.array([0.2, 0.1, -0.1, 0.0, 4.0], np.float32)
+        spec["projector"]["param"] = 50.0
+        return spec
+    if name == "hplt_n4":
+        v, f = sphere_hull(4, 800, seed=1)
+        spec = make_spec(4, v, f, screen=12, spp=8)
+        # a slanted three-dimensional wall beside the sphere
+        spec["hplt"] = {"org": np.array([1.35, -2.0, -2.0, -1.2], np.float32),
+                        "edges": np.array([[0, 4, 0, 0], [0, 0, 4, 0], [0.6, 0, 0, 3.0]], np.float32),
+                        "color": (0.8, 0.6, 0.5), "diffuse": 1.0}
+        return spec
+    if name == "two_mesh_n3":
+        bowl_v, bowl_f = sphere_hull(3, 400, seed=7, cap=0.9)  # open at the top
+        spec = make_spec(3, bowl_v, bowl_f, screen=24, spp=16, extent=5.0)
+        ball_v, ball_f = icosphere(2)
+        spec["mesh2"] = {"verts": (ball_v * np.float32(0.6) + np.array([1.5, 1.1, -0.4], np.float32)).astype(np.float32),
+                         "facets": ball_f, "color": (0.5, 0.7, 0.6), "diffuse": 1.0}
+        return spec
+    raise KeyError(name)
+
+
+def effective_spp(n: int, spp: int) -> int:
+    """Samples per pixel after stratification: the smallest k^(n-1) >= spp of the two integers around
+    spp^(1/(n-1)) (StratifiedJitteredSampler, src/painter/sampling/sampler.h:31-52); the library's
+    nt_effective_spp, restated so that processes that must not load the library can use it."""
+    m = n - 1
+    v = spp ** (1.0 / m)
+    f = math.floor(v)
+    return f ** m if f ** m >= spp else math.ceil(v) ** m
 
 
 def build_scene(spec: dict, threads: int = 0, tree_on_gpu: bool = False) -> ntrace.Scene:
@@ -166,9 +227,15 @@ def build_scene(spec: dict, threads: int = 0, tree_on_gpu: bool = False) -> ntra
         s.add_mesh(spec["verts"], spec["facets"], color=spec["mesh_color"], diffuse=spec["mesh_diffuse"])
         if spec.get("normals") is not None:
             s.set_mesh_normals(0, spec["normals"], spec.get("facet_normals"))
+    m2 = spec.get("mesh2")
+    if m2 is not None:
+        s.add_mesh(m2["verts"], m2["facets"], color=m2["color"], diffuse=m2["diffuse"])
     if spec["floor"] is not None:
         fl = spec["floor"]
         s.add_parallelotope(fl["org"], fl["edges"], color=fl["color"], diffuse=fl["diffuse"])
+    hp = spec.get("hplt")
+    if hp is not None:
+        s.add_hyperplane_parallelotope(hp["org"], hp["edges"], color=hp["color"], diffuse=hp["diffuse"])
     L = spec["light"]
     if L["kind"] == 0:
         s.add_point_light(L["pos"], L["color"], L["unit"])

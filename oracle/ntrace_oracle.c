@@ -393,6 +393,7 @@ static double now_seconds(void)
         {                                                                                                         \
                 int n = in->n;                                                                                    \
                 Mesh_##S* mesh = NULL;                                                                            \
+                Mesh_##S* mesh2 = NULL;                                                                           \
                 if (in->nfacets > 0)                                                                              \
                 {                                                                                                 \
                         mesh = mesh_build_##S(n, in->verts, in->nverts, in->facets, in->nfacets, err, errlen);   \
@@ -401,10 +402,21 @@ static double now_seconds(void)
                                 return 1;                                                                         \
                         }                                                                                         \
                 }                                                                                                 \
+                if (in->nfacets2 > 0)                                                                             \
+                {                                                                                                 \
+                        mesh2 = mesh_build_##S(n, in->verts2, in->nverts2, in->facets2, in->nfacets2, err,       \
+                                               errlen);                                                           \
+                        if (!mesh2)                                                                               \
+                        {                                                                                         \
+                                mesh_free_##S(mesh);                                                              \
+                                return 1;                                                                         \
+                        }                                                                                         \
+                }                                                                                                 \
                 Scene_##S scene;                                                                                  \
-                if (scene_make_##S(in, mesh, max_depth, &scene, err, errlen))                                     \
+                if (scene_make_##S(in, mesh, mesh2, max_depth, &scene, err, errlen))                              \
                 {                                                                                                 \
                         mesh_free_##S(mesh);                                                                      \
+                        mesh_free_##S(mesh2);                                                                     \
                         return 1;                                                                                 \
                 }                                                                                                 \
                 PaintJob_##S job;                                                                                 \
@@ -458,6 +470,7 @@ static double now_seconds(void)
                 free(scene.ntype);                                                                                \
                 free(scene.nsign);                                                                                \
                 mesh_free_##S(mesh);                                                                              \
+                mesh_free_##S(mesh2);                                                                             \
                 return 0;                                                                                         \
         }
 

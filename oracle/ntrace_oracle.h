@@ -64,6 +64,19 @@ typedef struct ort_scene
         const float* normals;
         long nnormals;
         const int* facet_normals;
+        /* optional second mesh (nfacets2 == 0: none), after the first in object order */
+        const float* verts2;
+        long nverts2;
+        const int* facets2;
+        long nfacets2;
+        float mesh2_color[3];
+        float mesh2_diffuse;
+        /* optional (n-1)-parallelotope in a hyperplane (has_hplt == 0: none), last in object order */
+        int has_hplt;
+        float hplt_org[6];
+        float hplt_edges[30];
+        float hplt_color[3];
+        float hplt_diffuse;
 } ort_scene;
 
 typedef struct ort_stats

@@ -8,7 +8,8 @@
 //       intersect_approximate + intersect_precise exactly as src/painter/shapes/test/test_mesh.cpp:139-152.
 //   refb_mesh_tree_*                    - the 2^N-tree that Mesh built (src/painter/space/tree.h:390-525).
 //   refb_paint                          - paint<N,T>() (src/painter/painter.cpp:599-625) on a scene made of
-//       the reference's own VisibleSharedMesh, VisibleParallelotope, VisiblePointLight/ConstantLight and
+//       the reference's own VisibleSharedMesh (one or two), VisibleParallelotope,
+//       VisibleHyperplaneParallelotope, VisiblePointLight/ConstantLight and
 //       VisibleParallel/Perspective/SphericalProjector (src/painter/visible_*.h).
 //
 // Two constants of painter.cpp are made adjustable without editing that file.  painter.cpp is
@@ -436,6 +437,19 @@ struct refb_scene
         const float* normals;
         long nnormals;
         const int* facet_normals;
+        // optional second mesh (nfacets2 == 0: none), after the first in object order
+        const float* verts2;
+        long nverts2;
+        const int* facets2;
+        long nfacets2;
+        float mesh2_color[3];
+        float mesh2_diffuse;
+        // optional (n-1)-parallelotope in a hyperplane (has_hplt == 0: none), last in object order
+        int has_hplt;
+        float hplt_org[6];
+        float hplt_edges[30];
+        float hplt_color[3];
+        float hplt_diffuse;
 };
 
 struct refb_stats
@@ -470,7 +484,9 @@ template <size_t N, typename T>
 class BridgeScene final : public PaintObjects<N, T>
 {
         std::unique_ptr<VisibleSharedMesh<N, T>> m_mesh;
+        std::unique_ptr<VisibleSharedMesh<N, T>> m_mesh2;
         std::unique_ptr<VisibleParallelotope<N, T>> m_floor;
+        std::unique_ptr<VisibleHyperplaneParallelotope<N, T>> m_hplt;
         std::unique_ptr<const LightSource<N, T>> m_light;
         std::unique_ptr<const Projector<N, T>> m_projector;
         SurfaceProperties<N, T> m_default;
@@ -485,8 +501,17 @@ class BridgeScene final : public PaintObjects<N, T>
                 return std::make_unique<VisibleParallelotope<N, T>>(org, e[I]...);
         }
 
+        template <size_t... I>
+        static std::unique_ptr<VisibleHyperplaneParallelotope<N, T>> make_hplt(const Vector<N, T>& org,
+                                                                              const std::array<Vector<N, T>, N - 1>& e,
+                                                                              std::index_sequence<I...>)
+        {
+                return std::make_unique<VisibleHyperplaneParallelotope<N, T>>(org, e[I]...);
+        }
+
 public:
-        BridgeScene(const refb_scene& s, std::shared_ptr<const Mesh<N, T>> mesh)
+        BridgeScene(const refb_scene& s, std::shared_ptr<const Mesh<N, T>> mesh,
+                    std::shared_ptr<const Mesh<N, T>> mesh2 = nullptr)
         {
                 if (mesh)
                 {
@@ -495,6 +520,14 @@ public:
                         m_mesh->set_diffuse_and_fresnel(s.mesh_diffuse, 0);
                         m_mesh->set_light_source(false);
                         m_objects.push_back(m_mesh.get());
+                }
+                if (mesh2)
+                {
+                        m_mesh2 = std::make_unique<VisibleSharedMesh<N, T>>(mesh2);
+                        m_mesh2->set_color(color_from(s.mesh2_color));
+                        m_mesh2->set_diffuse_and_fresnel(s.mesh2_diffuse, 0);
+                        m_mesh2->set_light_source(false);
+                        m_objects.push_back(m_mesh2.get());
                 }
                 if (s.has_floor)
                 {
@@ -508,6 +541,19 @@ public:
                         m_floor->set_diffuse_and_fresnel(s.floor_diffuse, 0);
                         m_floor->set_light_source(false);
                         m_objects.push_back(m_floor.get());
+                }
+                if (s.has_hplt)
+                {
+                        std::array<Vector<N, T>, N - 1> e;
+                        for (unsigned i = 0; i < N - 1; ++i)
+                        {
+                                e[i] = vec_from<N, T>(s.hplt_edges + i * N);
+                        }
+                        m_hplt = make_hplt(vec_from<N, T>(s.hplt_org), e, std::make_index_sequence<N - 1>());
+                        m_hplt->set_color(color_from(s.hplt_color));
+                        m_hplt->set_diffuse_and_fresnel(s.hplt_diffuse, 0);
+                        m_hplt->set_light_source(false);
+                        m_objects.push_back(m_hplt.get());
                 }
                 if (s.light_kind == 0)
                 {
@@ -684,7 +730,14 @@ int paint_impl(const refb_scene& s, int spp, int max_depth, unsigned long long s
                                                                     s.facet_normals));
                 mesh = static_cast<MeshHandle<N, T>*>(h.get())->mesh;
         }
-        BridgeScene<N, T> scene(s, mesh);
+        std::shared_ptr<const Mesh<N, T>> mesh2;
+        if (s.nfacets2 > 0)
+        {
+                std::unique_ptr<MeshHandleBase> h(
+                        mesh_create<N, T>(s.verts2, s.nverts2, s.facets2, s.nfacets2, std::max(1, s.tree_threads)));
+                mesh2 = static_cast<MeshHandle<N, T>*>(h.get())->mesh;
+        }
+        BridgeScene<N, T> scene(s, mesh, mesh2);
 
         std::array<int, M> size;
         for (unsigned i = 0; i < M; ++i)
