@@ -14,6 +14,13 @@ with the scene's arrays copied from pinned host memory and the image read back e
 --impl reference: the reference painter (oracle/_ref, compiled from the reference's own sources) on
 the host's cores, each step a seeded random pixel sample of the same frame.
 
+On one GPU the line also carries (skip with --no-extras):
+  per_n: the n = 3 (400^2, 16 spp, 20,480 triangles) and n = 5 (48^4, 16 spp after stratification,
+      1,541,774 4-simplices) configurations, measured the same way over 5 frames;
+  denoise_time_to_rmse_1e-2: per configuration, the time a whole frame needs to reach relative RMSE
+      1e-2 (on the centred window, against a 64k-sample render of it) plain and with the learned
+      denoiser (committed weights), on the k^(n-1) sample grid; the plain time fitted to the target.
+
 Multi-GPU (torchrun): every rank renders the whole frame with its own sample range (weak scaling);
 the per-pixel sums are combined with one NCCL all-reduce after the timed region.
 """
@@ -215,6 +222,159 @@ def mesh_block(spec: dict, hull: str) -> dict:
     return {"facets": int(len(spec["facets"])), "vertices": int(len(spec["verts"])), "hull": hull}
 
 
+def measure_plain(scene, spec: dict, args, steps: int, rank: int, world: int, local: int, dist,
+                  e2e: bool = True) -> dict:
+    """paths/s of the plain tracer on one built scene: autotuned pool, W warm-up frames (the last one
+    with per-kernel device events), K timed frames between two events on the scene's stream (max over
+    ranks), then K frames end to end through the public API."""
+    import torch
+
+    from math_b200 import distributed, scenes
+
+    n = spec["n"]
+    spp, depth = spec["spp"], spec["max_depth"]
+    stream = torch.cuda.ExternalStream(scene.stream)
+    # the library's autotuner picks the path-pool size and the iterations per graph launch from probe
+    # passes of this frame (untimed; it clears the accumulator)
+    tuned, _ = scene.autotune(spp, max_depth=depth, seed=spec["seed"])
+    # every rank traces the same Philox stream; ranks take disjoint sample ranges (pass k of rank r
+    # covers samples [(k * world + r) * spp_eff, + spp_eff)), so N ranks render N different passes
+    spp_eff = scenes.effective_spp(n, spp)
+
+    def offset(k: int) -> int:
+        return distributed.sample_offset(rank, k, spp_eff, world)
+
+    ropts = dict(max_depth=depth, seed=spec["seed"], pool_paths=tuned["pool_paths"],
+                 graph_iterations=tuned["graph_iterations"])
+
+    # warm-up (the last one is also the per-kernel timing pass: device events around every launch)
+    for _ in range(args.warmup - 1):
+        scene.render(spp, **ropts)
+    timed = scene.render(spp, **ropts, timing=True)
+    scene.clear()
+
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    stats = []
+    with ClockSampler(local) as clocks:
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for k in range(steps):
+            stats.append(scene.render(spp, **ropts, sample_offset=offset(k)))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+    ms = ev0.elapsed_time(ev1)
+    paths = sum(s["paths"] for s in stats)
+    ms_all = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    paths_all = torch.tensor([paths], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(ms_all, op=dist.ReduceOp.MAX)
+        dist.all_reduce(paths_all, op=dist.ReduceOp.SUM)
+    ms_max = float(ms_all.item())
+    out = {"value": float(paths_all.item()) / (ms_max / 1000.0), "ms_per_step": ms_max / steps, "steps": steps,
+           "paths_per_step": paths // max(1, steps), "launches": sum(s["launches"] for s in stats),
+           "device_errors": sum(s["error_bits"] for s in stats), "timed": timed, "tuned": tuned,
+           "clocks": clocks.summary()}
+
+    # combine the ranks' samples (disjoint sample ranges of one Philox stream) into one image: one NCCL
+    # all-reduce of the per-pixel sums, after the timed region
+    if dist:
+        img, spp_done = scene.image()
+        t0 = time.perf_counter()
+        distributed.combine(img, spp_done)
+        torch.cuda.synchronize()
+        out["combine_ms"] = 1000 * (time.perf_counter() - t0)
+
+    if e2e:
+        # end to end through the public API: every step's scene arrays cross from pinned host memory
+        # (double-buffered: step k+1's copy into the staging buffers runs on the scene's copy stream
+        # while step k renders, then moves into the live arrays on the device), every step's image is
+        # read back; wall clock around the calls, the first step's copy included
+        scene.clear()
+        host_img = torch.empty((scene.pixel_count, 3), dtype=torch.float32, pin_memory=True).numpy()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_paths = 0
+        h2d = scene.upload_begin()
+        for k in range(steps):
+            scene.upload_commit()
+            if k + 1 < steps:
+                scene.upload_begin()
+            st = scene.render(spp, **ropts, sample_offset=offset(k))
+            scene.image(out=host_img)
+            e2e_paths += st["paths"]
+        e2e_s = time.perf_counter() - t0
+        e2e_all = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+        if dist:
+            dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
+        out["e2e"] = {"value": e2e_paths * world / float(e2e_all.item()), "unit": "paths/s", "h2d_bytes_per_step": h2d,
+                      "d2h_bytes_per_step": host_img.nbytes, "steps": steps}
+    return out
+
+
+def roofline(n: int, timed: dict, name: str, pool_paths: int) -> dict:
+    """Roofline of the dominant walk kernel (the one with the larger device time) from the timing pass:
+    algorithmic bytes per launch (the reference algorithm's work counters, algorithmic_work) over the
+    launch's CUDA-event time, against the measured HBM copy peak."""
+    peaks = measured_peaks()
+    walks = {}
+    for kind, prefix in (("extend", ""), ("shadow", "shadow_")):
+        b, f = algorithmic_work(n, timed[prefix + "facet_tests"], timed[prefix + "box_steps"],
+                                timed[prefix + "descent_levels"])
+        launches_k = max(1, timed[kind + "_launches"])
+        ms = timed[kind + "_ms"] / launches_k
+        walks[kind] = {"bytes": b / launches_k, "flops": f / launches_k, "launch_ms": ms,
+                       "achieved": (b / launches_k) / (ms / 1000.0) / 1e9 if ms > 0 else 0.0}
+    dom = max(walks, key=lambda k: timed[k + "_ms"])
+    # DRAM bytes per launch from an ncu capture (profiles/traffic.json), scaled by the algorithmic bytes
+    # of this run's launches over those of the captured ones when the pool size differs (a launch's
+    # traffic grows with the rays it processes)
+    traffic = None
+    tf = ROOT / "profiles" / "traffic.json"
+    if tf.exists():
+        try:
+            t = json.loads(tf.read_text())
+            traffic = t.get(f"{name}_{dom}_bytes_per_launch")
+            alg = t.get(f"{name}_{dom}_algorithmic_bytes_per_launch")
+            if traffic is not None and t.get("pool_paths") != pool_paths:
+                traffic = traffic * walks[dom]["bytes"] / alg if alg else None
+        except Exception:
+            traffic = None
+    achieved = walks[dom]["achieved"]
+    return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+            "kernel": "k_shadow_refill" if dom == "shadow" else "k_extend_refill",
+            "peak_source": peaks["source"], "algorithmic_bytes_per_launch": walks[dom]["bytes"],
+            "algorithmic_flops_per_launch": walks[dom]["flops"], "launch_ms": walks[dom]["launch_ms"],
+            "walk_algorithmic_gbs": {k: w["achieved"] for k, w in walks.items()}}
+
+
+def measure_denoise(scene, n: int) -> dict:
+    """The other half of the metric: time to relative RMSE <= 1e-2 against a 64k-sample render, plain
+    versus denoised (the committed weights), on a held-out variation of the scene at its configuration
+    screen (math_b200.train_denoiser.time_to_rmse)."""
+    from math_b200 import denoise, train_denoiser
+
+    den = denoise.Denoiser.load(ROOT / "math_b200" / "weights" / f"denoiser_n{n}.npz")
+    r = train_denoiser.time_to_rmse(scene, den, n, 1e-2, seed=77 + n)
+
+    def met(points):
+        ok = [p for p in points if p["rmse"] <= 1e-2]
+        return {"spp": ok[0]["spp"], "ms": 1000 * ok[0]["seconds"], "rmse": ok[0]["rmse"]} if ok else None
+
+    return {"screen": r["screen"], "reference_window": r["reference_window"], "reference_spp": r["reference_spp"],
+            "plain": met(r["plain"]), "denoised": met(r["denoised"]),
+            "plain_fitted_ms": 1000 * r["plain_time_to_target_fitted"],
+            "speedup": r["speedup"], "speedup_vs_fitted": r["speedup_vs_fitted"],
+            "plain_points": [{"spp": p["spp"], "ms": 1000 * p["seconds"], "rmse": p["rmse"]} for p in r["plain"]],
+            "denoised_points": [{"spp": p["spp"], "ms": 1000 * p["seconds"], "rmse": p["rmse"],
+                                 "input_rmse": p["input_rmse"]} for p in r["denoised"]]}
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -224,6 +384,8 @@ def main() -> None:
     ap.add_argument("--config", choices=sorted(CONFIGS), default="n4")
     ap.add_argument("--cpu-paths", type=int, default=8_000_000, help="paths in the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the other dimensions' lines and the denoised-versus-plain measurement")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
 
@@ -248,154 +410,78 @@ def main() -> None:
     os.environ.setdefault("NTRACE_NO_BUILD", "1")
     from math_b200 import scenes
 
+    extras = rank == 0 and world == 1 and not args.no_extras
+    others = [c for c in ("n3", "n4", "n5") if c != args.config] if extras else []
+    # the other configurations' meshes (the n = 5 hull takes tens of seconds on the host) are prepared
+    # on a host thread while the headline configuration runs on the GPU
+    prepared: dict = {}
+
+    def prepare():
+        for c in others:
+            prepared[c] = scenes.config(c)
+
+    prep = threading.Thread(target=prepare, daemon=True)
+    prep.start()
+
     spec = scenes.config(args.config)
     n = spec["n"]
     scene = scenes.build_scene(spec, tree_on_gpu=True)
-    spp, depth = spec["spp"], spec["max_depth"]
-    stream = torch.cuda.ExternalStream(scene.stream)
-
-    # the library's autotuner picks the path-pool size and the iterations per graph launch from probe
-    # passes of this frame (untimed; it clears the accumulator)
-    tuned, _ = scene.autotune(spp, max_depth=depth, seed=spec["seed"])
-    # every rank traces the same Philox stream; ranks take disjoint sample ranges (pass k of rank r
-    # covers samples [(k * world + r) * spp_eff, + spp_eff)), so N ranks render N different passes
-    from math_b200 import distributed
-
-    spp_eff = scenes.effective_spp(n, spp)
-
-    def offset(k: int) -> int:
-        return distributed.sample_offset(rank, k, spp_eff, world)
-
-    ropts = dict(max_depth=depth, seed=spec["seed"], pool_paths=tuned["pool_paths"],
-                 graph_iterations=tuned["graph_iterations"])
-
-    # warm-up (also the per-kernel timing pass: device events around every launch)
-    for _ in range(args.warmup - 1):
-        scene.render(spp, **ropts)
-    timed = scene.render(spp, **ropts, timing=True)
-    scene.clear()
-
-    # timed region: K frames, device time between two events on the scene's stream
-    ev0 = torch.cuda.Event(enable_timing=True)
-    ev1 = torch.cuda.Event(enable_timing=True)
-    stats = []
-    with ClockSampler(local) as clocks:
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ev0.record(stream)
-        for k in range(args.steps):
-            stats.append(scene.render(spp, **ropts, sample_offset=offset(k)))
-        ev1.record(stream)
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-    ms = ev0.elapsed_time(ev1)
-    paths = sum(s["paths"] for s in stats)
-    launches = sum(s["launches"] for s in stats)
-    errors = sum(s["error_bits"] for s in stats)
-    ms_all = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    paths_all = torch.tensor([paths], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(ms_all, op=dist.ReduceOp.MAX)
-        dist.all_reduce(paths_all, op=dist.ReduceOp.SUM)
-    ms_max = float(ms_all.item())
-    value = float(paths_all.item()) / (ms_max / 1000.0)
-
-    # combine the ranks' samples (disjoint sample ranges of one Philox stream) into one image: one NCCL
-    # all-reduce of the per-pixel sums, after the timed region
-    combine_ms = None
-    if dist:
-        from math_b200 import distributed
-
-        img, spp_done = scene.image()
-        t0 = time.perf_counter()
-        distributed.combine(img, spp_done)
-        torch.cuda.synchronize()
-        combine_ms = 1000 * (time.perf_counter() - t0)
-
-    # end to end through the public API: every step's scene arrays cross from pinned host memory
-    # (double-buffered: step k+1's copy into the staging buffers runs on the scene's copy stream while
-    # step k renders, then moves into the live arrays on the device), every step's image is read back;
-    # wall clock around the calls, the first step's copy included
-    scene.clear()
-    e2e_steps = max(1, args.steps)
-    h2d = d2h = 0
-    host_img = torch.empty((scene.pixel_count, 3), dtype=torch.float32, pin_memory=True).numpy()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    e2e_paths = 0
-    h2d = scene.upload_begin()
-    for k in range(e2e_steps):
-        scene.upload_commit()
-        if k + 1 < e2e_steps:
-            scene.upload_begin()
-        st = scene.render(spp, **ropts, sample_offset=offset(k))
-        scene.image(out=host_img)
-        e2e_paths += st["paths"]
-        d2h = host_img.nbytes
-    e2e_s = time.perf_counter() - t0
-    e2e_all = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(e2e_all, op=dist.ReduceOp.MAX)
-    e2e_value = e2e_paths * world / float(e2e_all.item())
-
-    # roofline of the dominant walk kernel (the one with the larger device time), from the timed pass
-    peaks = measured_peaks()
-    walks = {}
-    for kind, prefix in (("extend", ""), ("shadow", "shadow_")):
-        b, f = algorithmic_work(n, timed[prefix + "facet_tests"], timed[prefix + "box_steps"],
-                                timed[prefix + "descent_levels"])
-        launches_k = max(1, timed[kind + "_launches"])
-        ms = timed[kind + "_ms"] / launches_k
-        walks[kind] = {"bytes": b / launches_k, "flops": f / launches_k, "launch_ms": ms,
-                       "achieved": (b / launches_k) / (ms / 1000.0) / 1e9 if ms > 0 else 0.0}
-    dom = max(walks, key=lambda k: timed[k + "_ms"])
-    # DRAM bytes per launch from an ncu capture (profiles/traffic.json), scaled by the algorithmic bytes
-    # of this run's launches over those of the captured ones when the pool size differs (a launch's
-    # traffic grows with the rays it processes)
-    traffic = None
-    tf = ROOT / "profiles" / "traffic.json"
-    if tf.exists():
-        try:
-            t = json.loads(tf.read_text())
-            traffic = t.get(f"{args.config}_{dom}_bytes_per_launch")
-            alg = t.get(f"{args.config}_{dom}_algorithmic_bytes_per_launch")
-            if traffic is not None and t.get("pool_paths") != tuned["pool_paths"]:
-                traffic = traffic * walks[dom]["bytes"] / alg if alg else None
-        except Exception:
-            traffic = None
-    achieved = walks[dom]["achieved"]
+    m = measure_plain(scene, spec, args, args.steps, rank, world, local, dist)
+    timed, tuned = m["timed"], m["tuned"]
 
     result = {
-        "metric": metric_name(n), "value": value, "unit": "paths/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "metric": metric_name(n), "value": m["value"], "unit": "paths/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": config_block(spec, args),
         "mesh": mesh_block(spec, "exact (nt_convex_hull)"),
         "tuning": {"pool_paths": tuned["pool_paths"], "graph_iterations": tuned["graph_iterations"],
                    "tuned_by": "nt_autotune"},
-        "e2e": {"value": e2e_value, "unit": "paths/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "steps": e2e_steps},
-        "gpu_launches": launches,
-        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-                     "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-                     "kernel": "k_shadow_refill" if dom == "shadow" else "k_extend_refill",
-                     "peak_source": peaks["source"],
-                     "algorithmic_bytes_per_launch": walks[dom]["bytes"],
-                     "algorithmic_flops_per_launch": walks[dom]["flops"],
-                     "launch_ms": walks[dom]["launch_ms"]},
+        "e2e": m["e2e"],
+        "gpu_launches": m["launches"],
+        "roofline": roofline(n, timed, args.config, tuned["pool_paths"]),
         "kernels_ms_per_frame": {"raygen": timed["raygen_ms"], "extend": timed["extend_ms"], "shade": timed["shade_ms"],
                                  "shadow": timed["shadow_ms"]},
-        "walk_algorithmic_gbs": {k: w["achieved"] for k, w in walks.items()},
         "counters_per_frame": {k: timed[k] for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests",
                                                      "descent_levels", "shadow_facet_tests", "shadow_box_steps",
                                                      "shadow_retests", "shadow_descent_levels")},
-        "clocks": clocks.summary(),
-        "device_errors": errors,
+        "clocks": m["clocks"],
+        "device_errors": m["device_errors"],
     }
-    if combine_ms is not None:
-        result["combine_ms"] = combine_ms
+    if "combine_ms" in m:
+        result["combine_ms"] = m["combine_ms"]
+    if extras:
+        # the other dimensions (fewer steps) and the denoised-versus-plain time to the target error
+        denoise_res = {}
+        try:
+            denoise_res[args.config] = measure_denoise(scene, n)
+        except Exception as e:  # report it; the headline line stands
+            denoise_res[args.config] = {"error": repr(e)}
+        scene.close()
+        prep.join()
+        per_n = {}
+        for c in others:
+            sp = prepared[c]
+            sc = scenes.build_scene(sp, tree_on_gpu=True)
+            k = min(args.steps, 5)
+            mm = measure_plain(sc, sp, args, k, rank, world, local, dist)
+            per_n[c] = {"metric": metric_name(sp["n"]), "value": mm["value"], "unit": "paths/s",
+                        "ms_per_step": mm["ms_per_step"], "steps": k, "e2e": mm["e2e"],
+                        "config": config_block(sp, argparse.Namespace(config=c)),
+                        "mesh": mesh_block(sp, "exact (nt_convex_hull)"),
+                        "tuning": {"pool_paths": mm["tuned"]["pool_paths"],
+                                   "graph_iterations": mm["tuned"]["graph_iterations"]},
+                        "roofline": roofline(sp["n"], mm["timed"], c, mm["tuned"]["pool_paths"]),
+                        "kernels_ms_per_frame": {kk: mm["timed"][kk + "_ms"] for kk in ("raygen", "extend", "shade",
+                                                                                        "shadow")},
+                        "clocks": mm["clocks"], "device_errors": mm["device_errors"]}
+            try:
+                denoise_res[c] = measure_denoise(sc, sp["n"])
+            except Exception as e:
+                denoise_res[c] = {"error": repr(e)}
+            sc.close()
+        result["per_n"] = per_n
+        result["denoise_time_to_rmse_1e-2"] = denoise_res
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         result["cpu_baseline"] = cpu_baseline(spec, args.cpu_paths, os.cpu_count() or 1)
         # the same painter on one thread, over an eighth of the sample

@@ -507,7 +507,9 @@ enum TestResult : int
         T_UNSURE = 2
 };
 
-template <int N>
+// STAGED: the record lies in shared memory (staged by cp.async, leaf_closest_warp) and is read with
+// plain loads; otherwise it is read from global memory through the read-only path.
+template <int N, bool STAGED = false>
 __device__ __forceinline__ int facet_test32(const float4* rec, const Ray<N>& r, float ao, float* t_out)
 {
         constexpr float EPS = 5.9604645e-08f;  // 2^-24
@@ -523,7 +525,7 @@ __device__ __forceinline__ int facet_test32(const float4* rec, const Ray<N>& r, 
 #pragma unroll
         for (int q = 0; q < HEAD4; ++q)
         {
-                float4 v = __ldg(rec + q);
+                float4 v = STAGED ? rec[q] : __ldg(rec + q);
                 f[4 * q + 0] = v.x;
                 f[4 * q + 1] = v.y;
                 f[4 * q + 2] = v.z;
@@ -571,7 +573,7 @@ __device__ __forceinline__ int facet_test32(const float4* rec, const Ray<N>& r, 
 #pragma unroll
                 for (int q = first4; q < need4; ++q)
                 {
-                        float4 v = __ldg(rec + q);
+                        float4 v = STAGED ? rec[q] : __ldg(rec + q);
                         f[4 * q + 0] = v.x;
                         f[4 * q + 1] = v.y;
                         f[4 * q + 2] = v.z;
@@ -1277,6 +1279,41 @@ __device__ __forceinline__ PoolSlot* warp_pool()
         return s_pool + (threadIdx.x >> 5) * POOL_SLOTS;
 }
 
+// Facet records staged through shared memory.  A warp handles its pooled tests in chunks of
+// Stage<N>::SLOTS: it first reads the chunk's facet indices (ROUNDS independent loads per lane), then
+// copies their records into its staging slots with cp.async (ROUNDS x F4 16-byte copies per lane in
+// flight at once), waits once, and tests from shared memory.  A chunk costs two memory round trips
+// instead of two per 32 tests.  The buffer is dynamic shared memory (Stage<N>::BYTES per block of
+// WALK_BLOCK threads), at most 8 KB per warp.
+template <int N>
+struct Stage
+{
+        static constexpr int REC_BYTES = Rec32<N>::F4 * 16;
+        static constexpr int FIT = 8192 / (32 * REC_BYTES);
+        static constexpr int ROUNDS = FIT < 1 ? 1 : (FIT > 4 ? 4 : FIT);
+        static constexpr int SLOTS = 32 * ROUNDS;
+        static constexpr int BYTES = (WALK_BLOCK / 32) * SLOTS * REC_BYTES;
+        static_assert(SLOTS <= POOL_SLOTS, "a chunk's outcomes must fit the warp's pool");
+};
+
+__device__ __forceinline__ float4* stage_base()
+{
+        extern __shared__ float4 g_walk_stage[];
+        return g_walk_stage;
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+        const uint32_t a = (uint32_t)__cvta_generic_to_shared(smem);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all()
+{
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+
 // Closest facet of this lane's leaf (facets leaf_idx[start .. start + cnt)); every lane of the warp
 // calls it, lanes without a leaf with cnt = 0.  raw_org/raw_dir: the caller's raw rays for the
 // FP64 re-test of the fixed-ray-set query (null when rendering: the FP32 ray is promoted).
@@ -1309,13 +1346,21 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                 return best;
         }
         PoolSlot* pool = warp_pool();
+        constexpr int R = Stage<N>::ROUNDS;
+        constexpr int F4 = Rec32<N>::F4;
+        float4* const stage = stage_base() + (size_t)(threadIdx.x >> 5) * Stage<N>::SLOTS * F4;
         const Ray64Source<N> own_src{raw_org, raw_dir, raw};
-        for (int cb = 0; cb < total; cb += POOL_SLOTS)
+        for (int cb = 0; cb < total; cb += Stage<N>::SLOTS)
         {
-                const int ce = min(total, cb + POOL_SLOTS);
-                for (int k0 = cb; k0 < ce; k0 += 32)
+                const int ce = min(total, cb + Stage<N>::SLOTS);
+                // the chunk's facet indices (independent loads), then their records into the staging
+                // slots (all copies in flight at once)
+                int own[R];
+                int fid[R];
+#pragma unroll
+                for (int r = 0; r < R; ++r)
                 {
-                        const int k = k0 + lane;
+                        const int k = cb + 32 * r + lane;
                         // owner: the last lane whose list starts at or before k
                         int o = 0;
 #pragma unroll
@@ -1327,25 +1372,48 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                                         o += step;
                                 }
                         }
+                        own[r] = o;
                         const int o_start = __shfl_sync(full, start, o);
                         const int o_excl = __shfl_sync(full, excl, o);
+                        fid[r] = (k < ce) ? __ldg(&M.leaf_idx[o_start + (k - o_excl)]) : -1;
+                }
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                {
+                        if (fid[r] >= 0)
+                        {
+                                const float4* src = M.rec32 + (size_t)fid[r] * F4;
+                                float4* dst = stage + (size_t)(32 * r + lane) * F4;
+#pragma unroll
+                                for (int q = 0; q < F4; ++q)
+                                {
+                                        cp_async16(dst + q, src + q);
+                                }
+                        }
+                }
+                cp_async_wait_all();
+#pragma unroll
+                for (int r = 0; r < R; ++r)
+                {
+                        const int k = cb + 32 * r + lane;
+                        const int o = own[r];
                         const float o_ao = __shfl_sync(full, ao, o);
-                        Ray<N> r;
+                        Ray<N> rr;
 #pragma unroll
                         for (int i = 0; i < N; ++i)
                         {
-                                r.org[i] = __shfl_sync(full, ray.org[i], o);
-                                r.dir[i] = __shfl_sync(full, ray.dir[i], o);
+                                rr.org[i] = __shfl_sync(full, ray.org[i], o);
+                                rr.dir[i] = __shfl_sync(full, ray.dir[i], o);
                         }
                         const long long o_raw = raw_org ? __shfl_sync(full, raw, o) : 0;
                         if (k < ce)
                         {
-                                const int f = __ldg(&M.leaf_idx[o_start + (k - o_excl)]);
+                                const int f = fid[r];
                                 ++ws->facet_tests;
                                 float t = -1.0f;
                                 double t64 = -1.0;
                                 int keep = -1;
-                                int res = facet_test32<N>(M.rec32 + (size_t)f * Rec32<N>::F4, r, o_ao, &t);
+                                int res = facet_test32<N, true>(stage + (size_t)(32 * r + lane) * F4, rr, o_ao, &t);
                                 if (res == T_HIT)
                                 {
                                         keep = f;
@@ -1364,7 +1432,7 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                                         else
                                         {
                                                 ++ws->retests;
-                                                t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, r,
+                                                t64 = retest_facet<N>(M.rec64 + (size_t)f * Rec64<N>::DOUBLES, rr,
                                                                       Ray64Source<N>{raw_org, raw_dir, o_raw});
                                                 if (t64 > 0)
                                                 {

@@ -1083,12 +1083,16 @@ long long grid_for(long long count)
 // Resident blocks of a persistent kernel on this device (all SMs, as many blocks per SM as its
 // registers and shared memory allow).
 template <typename K>
-long long resident_blocks(K kernel)
+long long resident_blocks(K kernel, int dynamic_smem = 0)
 {
         int dev = 0, sms = 0, per_sm = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, 0);
+        if (dynamic_smem > 0)
+        {
+                cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, dynamic_smem);
+        }
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, BLOCK, dynamic_smem);
         return (long long)std::max(1, sms) * std::max(1, per_sm);
 }
 }
@@ -1148,8 +1152,9 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
 {
         static const long long extend_blocks = resident_blocks(k_extend<N>);
         static const long long shadow_blocks = resident_blocks(k_shadow<N>);
-        static const long long extend_refill_blocks = resident_blocks(k_extend_refill<N>);
-        static const long long shadow_refill_blocks = resident_blocks(k_shadow_refill<N>);
+        // the refill kernels stage facet records in dynamic shared memory (leaf_closest_warp)
+        static const long long extend_refill_blocks = resident_blocks(k_extend_refill<N>, Stage<N>::BYTES);
+        static const long long shadow_refill_blocks = resident_blocks(k_shadow_refill<N>, Stage<N>::BYTES);
         static const long long stream_blocks = resident_blocks(k_shade<N>);
         // scenes with exactly one mesh use the lane-refill walk kernels
         const bool one_mesh = S.nmesh == 1;
@@ -1178,7 +1183,7 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (one_mesh)
         {
-                k_extend_refill<N><<<ext_grid, BLOCK, 0, st>>>(S, A, H, counters);
+                k_extend_refill<N><<<ext_grid, BLOCK, Stage<N>::BYTES, st>>>(S, A, H, counters);
         }
         else
         {
@@ -1195,7 +1200,7 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (one_mesh)
         {
-                k_shadow_refill<N><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, counters);
+                k_shadow_refill<N><<<sh_grid, BLOCK, Stage<N>::BYTES, st>>>(S, SQ, accum, counters);
         }
         else
         {
@@ -1356,7 +1361,15 @@ cudaError_t launch_trace_closest(const MeshDev<N>& M, const float* org, const fl
         {
                 return cudaSuccess;
         }
-        k_trace_closest<N><<<(unsigned)grid_for<N>(nrays), BLOCK, 0, st>>>(M, org, dir, nrays, retest, facet, t, counters);
+        static const bool smem_set =
+                cudaFuncSetAttribute(k_trace_closest<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, Stage<N>::BYTES) ==
+                cudaSuccess;
+        if (!smem_set)
+        {
+                return cudaErrorInvalidValue;
+        }
+        k_trace_closest<N><<<(unsigned)grid_for<N>(nrays), BLOCK, Stage<N>::BYTES, st>>>(M, org, dir, nrays, retest, facet, t,
+                                                                                         counters);
         return cudaGetLastError();
 }
 
