@@ -1145,17 +1145,35 @@ void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
         }
 }
 
+// Resident blocks of every kernel of an iteration, and the dynamic shared memory of the walk kernels
+// (they stage facet records there, leaf_closest_warp): computed once per dimension, on the first call,
+// which the host makes before any capture (prepare_pass, nt_render_noalloc).
+template <int N>
+const LaunchSizes& Wavefront<N>::prepare()
+{
+        static const LaunchSizes sizes = []() {
+                LaunchSizes z;
+                z.extend_blocks = resident_blocks(k_extend<N>);
+                z.shadow_blocks = resident_blocks(k_shadow<N>);
+                z.extend_refill_blocks = resident_blocks(k_extend_refill<N>, Stage<N>::BYTES);
+                z.shadow_refill_blocks = resident_blocks(k_shadow_refill<N>, Stage<N>::BYTES);
+                z.stream_blocks = resident_blocks(k_shade<N>);
+                return z;
+        }();
+        return sizes;
+}
+
 template <int N>
 void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, double* accum, unsigned long long* counters,
                                      long long total_paths, int parity, cudaStream_t st, KernelTimes* times,
                                      cudaEvent_t* ev) const
 {
-        static const long long extend_blocks = resident_blocks(k_extend<N>);
-        static const long long shadow_blocks = resident_blocks(k_shadow<N>);
-        // the refill kernels stage facet records in dynamic shared memory (leaf_closest_warp)
-        static const long long extend_refill_blocks = resident_blocks(k_extend_refill<N>, Stage<N>::BYTES);
-        static const long long shadow_refill_blocks = resident_blocks(k_shadow_refill<N>, Stage<N>::BYTES);
-        static const long long stream_blocks = resident_blocks(k_shade<N>);
+        const LaunchSizes& L = prepare();
+        const long long extend_blocks = L.extend_blocks;
+        const long long shadow_blocks = L.shadow_blocks;
+        const long long extend_refill_blocks = L.extend_refill_blocks;
+        const long long shadow_refill_blocks = L.shadow_refill_blocks;
+        const long long stream_blocks = L.stream_blocks;
         // scenes with exactly one mesh use the lane-refill walk kernels
         const bool one_mesh = S.nmesh == 1;
         const bool smooth = S.smooth_normal != 0;
@@ -1233,6 +1251,7 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
         {
                 return cudaErrorInvalidValue;  // the pool was carved without the smooth-normal queue
         }
+        prepare();  // kernel attributes and occupancy, outside the capture below
         // iterations between host checks of the done flag (a pass takes tens of iterations; the few
         // that run after it is done find empty queues and return at once)
         const int BATCH = std::max(1, batch);

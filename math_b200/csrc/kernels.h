@@ -24,6 +24,16 @@ struct KernelTimes
         long long shadow_rays = 0;
 };
 
+// Grid sizes of an iteration's kernels (resident blocks on the whole device).
+struct LaunchSizes
+{
+        long long extend_blocks = 1;
+        long long shadow_blocks = 1;
+        long long extend_refill_blocks = 1;
+        long long shadow_refill_blocks = 1;
+        long long stream_blocks = 1;
+};
+
 // Wavefront path pool: path state A/B (double-buffered, compacted every bounce), the hit record and
 // the shadow-ray queue, all carved out of one caller-provided device allocation.
 template <int N>
@@ -72,6 +82,11 @@ struct Wavefront
         {
                 return 6 + (smooth ? 1 : 0);
         }
+
+        // The iteration kernels' attributes (dynamic shared memory of the walk kernels) and grid sizes,
+        // set up on the first call for this dimension.  Call it before capturing iterations into a
+        // graph (run() and the batch do).
+        static const LaunchSizes& prepare();
 };
 
 // Denoiser inputs: first-hit normal and depth of every pixel-centre camera ray; per-pixel mean and

@@ -1362,6 +1362,7 @@ template <int N>
 std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, const PassTarget& target = PassTarget())
 {
         double* const moments_accum = target.moments;
+        Wavefront<N>::prepare();  // kernel attributes before any capture of the pass's iterations
         auto job = std::make_unique<PassJobN<N>>();
         job->t0 = std::chrono::steady_clock::now();
         job->s = s;
