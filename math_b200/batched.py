@@ -70,7 +70,7 @@ def main(argv=None) -> None:
     for sp in specs:
         t = tuned[sp["n"]]
         opts.append(dict(samples_per_pixel=sp["spp"], max_depth=5, seed=sp["seed"], pool_paths=t["pool_paths"],
-                         graph_iterations=t["graph_iterations"]))
+                         graph_iterations=t["graph_iterations"], walk_chunk=t["walk_chunk"]))
     paths = sum(s.pixel_count * ntrace.effective_spp(sp["n"], sp["spp"]) for s, sp in zip(built, specs))
     # warm-up, then timed passes
     ntrace.render_batch(built, opts)

@@ -1285,12 +1285,21 @@ __device__ __forceinline__ PoolSlot* warp_pool()
 // flight at once), waits once, and tests from shared memory.  A chunk costs two memory round trips
 // instead of two per 32 tests.  The buffer is dynamic shared memory (Stage<N>::BYTES per block of
 // WALK_BLOCK threads), at most 8 KB per warp.
+// Other chunk sizes (R = 1, 2 or 4 rounds) are compiled as kernel variants that the autotuner
+// chooses from (nt_render_opts.walk_chunk).
 template <int N>
-struct Stage
+struct StageFit
 {
         static constexpr int REC_BYTES = Rec32<N>::F4 * 16;
         static constexpr int FIT = 8192 / (32 * REC_BYTES);
-        static constexpr int ROUNDS = FIT < 1 ? 1 : (FIT > 4 ? 4 : FIT);
+        static constexpr int ROUNDS = FIT < 1 ? 1 : (FIT > 4 ? 4 : (FIT == 3 ? 2 : FIT));
+};
+
+template <int N, int R = StageFit<N>::ROUNDS>
+struct Stage
+{
+        static constexpr int REC_BYTES = Rec32<N>::F4 * 16;
+        static constexpr int ROUNDS = R;
         static constexpr int SLOTS = 32 * ROUNDS;
         static constexpr int BYTES = (WALK_BLOCK / 32) * SLOTS * REC_BYTES;
         static_assert(SLOTS <= POOL_SLOTS, "a chunk's outcomes must fit the warp's pool");
@@ -1317,7 +1326,7 @@ __device__ __forceinline__ void cp_async_wait_all()
 // Closest facet of this lane's leaf (facets leaf_idx[start .. start + cnt)); every lane of the warp
 // calls it, lanes without a leaf with cnt = 0.  raw_org/raw_dir: the caller's raw rays for the
 // FP64 re-test of the fixed-ray-set query (null when rendering: the FP32 ray is promoted).
-template <int N>
+template <int N, int RR = StageFit<N>::ROUNDS>
 __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start, int cnt, const Ray<N>& ray, float ao,
                                                  long long raw, const float* raw_org, const float* raw_dir, int retest,
                                                  float* t_best, WalkStats* ws)
@@ -1346,13 +1355,13 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                 return best;
         }
         PoolSlot* pool = warp_pool();
-        constexpr int R = Stage<N>::ROUNDS;
+        constexpr int R = RR;
         constexpr int F4 = Rec32<N>::F4;
-        float4* const stage = stage_base() + (size_t)(threadIdx.x >> 5) * Stage<N>::SLOTS * F4;
+        float4* const stage = stage_base() + (size_t)(threadIdx.x >> 5) * Stage<N, R>::SLOTS * F4;
         const Ray64Source<N> own_src{raw_org, raw_dir, raw};
-        for (int cb = 0; cb < total; cb += Stage<N>::SLOTS)
+        for (int cb = 0; cb < total; cb += Stage<N, R>::SLOTS)
         {
-                const int ce = min(total, cb + Stage<N>::SLOTS);
+                const int ce = min(total, cb + Stage<N, R>::SLOTS);
                 // the chunk's facet indices (independent loads), then their records into the staging
                 // slots (all copies in flight at once)
                 int own[R];
@@ -1521,7 +1530,7 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
 
 // walk_step with the leaf's facets tested by leaf_closest_warp.  Every lane of the warp calls it
 // (active = false for lanes without a walk, whose result is ignored).
-template <int N>
+template <int N, int RR = StageFit<N>::ROUNDS>
 __device__ __forceinline__ int walk_step_warp(const MeshDev<N>& M, Walk<N>& w, bool active, int retest,
                                               const float* raw_org, const float* raw_dir, float* t_out, int* facet_out,
                                               WalkStats* ws)
@@ -1560,7 +1569,7 @@ __device__ __forceinline__ int walk_step_warp(const MeshDev<N>& M, Walk<N>& w, b
         }
         const int cnt = (leaf && nd.y > 0) ? nd.y : 0;
         float t = FLT_MAX;
-        const int f = leaf_closest_warp<N>(M, nd.x, cnt, w.ray, w.ao, w.raw, raw_org, raw_dir, retest, &t, ws);
+        const int f = leaf_closest_warp<N, RR>(M, nd.x, cnt, w.ray, w.ao, w.raw, raw_org, raw_dir, retest, &t, ws);
         if (status != W_RUNNING)
         {
                 return status;

@@ -138,6 +138,8 @@ struct DevScene
         int smooth_normal;
         int max_depth;
         int retest;          // 1: FP64 re-test of uncertain facet tests
+        int walk_rounds;     // walk kernels: rounds of 32 pooled facet tests staged per warp chunk (1, 2
+                             // or 4; 0: the default for N); host-side choice of the kernel variant
 };
 
 // Render-pass constants.

@@ -701,7 +701,8 @@ __device__ __forceinline__ long long lane_refill(bool idle, unsigned long long* 
 }
 
 // Extension rays of a scene with one mesh: closest_plan at fetch, then one leaf per iteration.
-template <int N>
+// R: rounds of 32 pooled facet tests staged per warp chunk (Stage<N, R>).
+template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, unsigned long long* counters)
 {
@@ -764,7 +765,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                 {
                         float t = 0;
                         int f = -1;
-                        int status = walk_step_warp<N>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
+                        int status = walk_step_warp<N, R>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
                         if (i >= 0 && status != W_RUNNING)
                         {
                                 float tt;
@@ -789,7 +790,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
 
 // Shadow rays of a scene with one mesh: a non-mesh object nearer than the light occludes at once;
 // otherwise the mesh is walked (up to the light's distance) when its root box starts before the light.
-template <int N>
+template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, unsigned long long* counters)
 {
@@ -869,7 +870,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                 {
                         float t = 0;
                         int f = -1;
-                        int status = walk_step_warp<N>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
+                        int status = walk_step_warp<N, R>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
                         if (i >= 0 && status != W_RUNNING)
                         {
                                 if (!(status == W_HIT && t < dist))
@@ -1155,8 +1156,12 @@ const LaunchSizes& Wavefront<N>::prepare()
                 LaunchSizes z;
                 z.extend_blocks = resident_blocks(k_extend<N>);
                 z.shadow_blocks = resident_blocks(k_shadow<N>);
-                z.extend_refill_blocks = resident_blocks(k_extend_refill<N>, Stage<N>::BYTES);
-                z.shadow_refill_blocks = resident_blocks(k_shadow_refill<N>, Stage<N>::BYTES);
+                z.extend_refill_blocks[0] = resident_blocks(k_extend_refill<N, 1>, Stage<N, 1>::BYTES);
+                z.extend_refill_blocks[1] = resident_blocks(k_extend_refill<N, 2>, Stage<N, 2>::BYTES);
+                z.extend_refill_blocks[2] = resident_blocks(k_extend_refill<N, 4>, Stage<N, 4>::BYTES);
+                z.shadow_refill_blocks[0] = resident_blocks(k_shadow_refill<N, 1>, Stage<N, 1>::BYTES);
+                z.shadow_refill_blocks[1] = resident_blocks(k_shadow_refill<N, 2>, Stage<N, 2>::BYTES);
+                z.shadow_refill_blocks[2] = resident_blocks(k_shadow_refill<N, 4>, Stage<N, 4>::BYTES);
                 z.stream_blocks = resident_blocks(k_shade<N>);
                 return z;
         }();
@@ -1171,8 +1176,11 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         const LaunchSizes& L = prepare();
         const long long extend_blocks = L.extend_blocks;
         const long long shadow_blocks = L.shadow_blocks;
-        const long long extend_refill_blocks = L.extend_refill_blocks;
-        const long long shadow_refill_blocks = L.shadow_refill_blocks;
+        // the walk kernels' staging chunk: 1, 2 or 4 rounds of 32 pooled tests per warp
+        const int rounds = S.walk_rounds > 0 ? S.walk_rounds : StageFit<N>::ROUNDS;
+        const int vi = rounds >= 4 ? 2 : (rounds >= 2 ? 1 : 0);
+        const long long extend_refill_blocks = L.extend_refill_blocks[vi];
+        const long long shadow_refill_blocks = L.shadow_refill_blocks[vi];
         const long long stream_blocks = L.stream_blocks;
         // scenes with exactly one mesh use the lane-refill walk kernels
         const bool one_mesh = S.nmesh == 1;
@@ -1201,7 +1209,18 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (one_mesh)
         {
-                k_extend_refill<N><<<ext_grid, BLOCK, Stage<N>::BYTES, st>>>(S, A, H, counters);
+                if (vi == 0)
+                {
+                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, counters);
+                }
+                else if (vi == 1)
+                {
+                        k_extend_refill<N, 2><<<ext_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, A, H, counters);
+                }
+                else
+                {
+                        k_extend_refill<N, 4><<<ext_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, A, H, counters);
+                }
         }
         else
         {
@@ -1218,7 +1237,18 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (one_mesh)
         {
-                k_shadow_refill<N><<<sh_grid, BLOCK, Stage<N>::BYTES, st>>>(S, SQ, accum, counters);
+                if (vi == 0)
+                {
+                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, counters);
+                }
+                else if (vi == 1)
+                {
+                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, counters);
+                }
+                else
+                {
+                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, counters);
+                }
         }
         else
         {

@@ -29,8 +29,8 @@ struct LaunchSizes
 {
         long long extend_blocks = 1;
         long long shadow_blocks = 1;
-        long long extend_refill_blocks = 1;
-        long long shadow_refill_blocks = 1;
+        long long extend_refill_blocks[3] = {1, 1, 1};  // per staging chunk: 1, 2, 4 rounds of 32 tests
+        long long shadow_refill_blocks[3] = {1, 1, 1};
         long long stream_blocks = 1;
 };
 

@@ -1340,6 +1340,16 @@ struct PassJobN final : PassJob
         }
 };
 
+// The walk kernels' staging chunk in rounds of 32 tests (nt_render_opts.walk_chunk; 0: the default).
+int walk_rounds(const nt_render_opts& o)
+{
+        if (o.walk_chunk != 0 && o.walk_chunk != 32 && o.walk_chunk != 64 && o.walk_chunk != 128)
+        {
+                fail(NT_EINVAL, "walk_chunk must be 0, 32, 64 or 128");
+        }
+        return o.walk_chunk / 32;
+}
+
 // Where a pass's radiance goes when it is not the scene's per-pixel accumulator.
 struct PassTarget
 {
@@ -1385,6 +1395,7 @@ std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, cons
         std::memcpy(&S, s->dev_scene.data(), sizeof(S));
         S.max_depth = o.max_depth;
         S.retest = o.retest;
+        S.walk_rounds = walk_rounds(o);
         const bool smooth = smooth_shading(s, o);
         S.smooth_normal = smooth ? 1 : 0;
         const long long npix = s->pixel_count();
@@ -1556,6 +1567,7 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
         S.max_depth = o.max_depth;
         S.retest = o.retest;
         S.smooth_normal = smooth ? 1 : 0;
+        S.walk_rounds = walk_rounds(o);
         unsigned long long* counters = static_cast<unsigned long long*>(scratch);
         Wavefront<N> W;
         W.carve(static_cast<char*>(scratch) + head, Q, lights, smooth);
@@ -2565,6 +2577,27 @@ int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tun
                                                 best_t = ms;
                                                 best = o;
                                         }
+                                }
+                        }
+                }
+                // then the walk kernels' staging chunk at the best pool and iterations
+                const nt_render_opts at = best;
+                for (int chunk : {32, 64, 128})
+                {
+                        nt_render_opts o = at;
+                        o.walk_chunk = chunk;
+                        o.timing = 0;
+                        o.stop = nullptr;
+                        for (int rep = 0; rep < 2; ++rep)
+                        {
+                                auto t0 = std::chrono::steady_clock::now();
+                                dispatch<RenderF>(scene->n, scene, o, (nt_stats*)nullptr);
+                                const double ms =
+                                        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+                                if (rep == 1 && ms < best_t)
+                                {
+                                        best_t = ms;
+                                        best = o;
                                 }
                         }
                 }

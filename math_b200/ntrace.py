@@ -63,7 +63,7 @@ class RenderOpts(ctypes.Structure):
     _fields_ = [("samples_per_pixel", ctypes.c_int), ("max_depth", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("retest", ctypes.c_int), ("smooth_normal", ctypes.c_int), ("pool_paths", ctypes.c_int64),
                 ("timing", ctypes.c_int), ("stop", ctypes.c_void_p), ("graph_iterations", ctypes.c_int),
-                ("sample_offset", ctypes.c_int64)]
+                ("sample_offset", ctypes.c_int64), ("walk_chunk", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -212,10 +212,10 @@ def cosine_sphere_coefficient(n: int) -> float:
 
 def render_opts(samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                 smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False,
-                graph_iterations: int = 0, sample_offset: int = 0) -> RenderOpts:
+                graph_iterations: int = 0, sample_offset: int = 0, walk_chunk: int = 0) -> RenderOpts:
     return RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)),
                       int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None, int(graph_iterations),
-                      int(sample_offset))
+                      int(sample_offset), int(walk_chunk))
 
 
 def render_batch(scenes: list, opts: list[dict]) -> list[dict]:
@@ -355,11 +355,11 @@ class Scene:
 
     def render(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None,
-               graph_iterations: int = 0, sample_offset: int = 0) -> dict:
+               graph_iterations: int = 0, sample_offset: int = 0, walk_chunk: int = 0) -> dict:
         """One pass added to the accumulator (nt_render); sample_offset > 0 starts it at that sample
         index, 0 continues after the accumulated samples."""
         o = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, pool_paths, timing,
-                        graph_iterations, sample_offset)
+                        graph_iterations, sample_offset, walk_chunk)
         if stop is not None:
             o.stop = ctypes.cast(stop, ctypes.c_void_p)
         st = Stats()
@@ -386,13 +386,15 @@ class Scene:
 
     def autotune(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                  smooth_normal: bool = False) -> tuple[dict, float]:
-        """Fastest pool size and iterations per graph launch for passes of samples_per_pixel (probe
-        passes; clears the accumulator).  Returns ({pool_paths, graph_iterations}, pass ms)."""
+        """Fastest pool size, iterations per graph launch and walk staging chunk for passes of
+        samples_per_pixel (probe passes; clears the accumulator).  Returns ({pool_paths,
+        graph_iterations, walk_chunk}, pass ms)."""
         base = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, 0, False, 0)
         out = RenderOpts()
         ms = ctypes.c_double()
         _check(self._lib.nt_autotune(self._h, ctypes.byref(base), ctypes.byref(out), ctypes.byref(ms)))
-        return {"pool_paths": int(out.pool_paths), "graph_iterations": int(out.graph_iterations)}, float(ms.value)
+        return {"pool_paths": int(out.pool_paths), "graph_iterations": int(out.graph_iterations),
+                "walk_chunk": int(out.walk_chunk)}, float(ms.value)
 
     def clear(self) -> None:
         _check(self._lib.nt_accum_clear(self._h))

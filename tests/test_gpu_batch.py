@@ -40,6 +40,35 @@ def test_graph_and_direct_iterations_trace_the_same_paths(require_gpu):
         assert rrmse(img, img_d) < 1e-12, it
 
 
+@pytest.mark.parametrize("name", ["n3_small", "n4_small", "n5_small", "n6_small"])
+def test_walk_chunks_trace_the_same_paths(require_gpu, name):
+    """The walk kernels' staging chunk (32, 64 or 128 pooled facet tests per warp) is a tuning choice
+    only: every chunk makes the same decisions (same work counters, same image)."""
+    spec, s = _scene(name)
+    ref = None
+    for chunk in (32, 64, 128):
+        s.clear()
+        st = s.render(spec["spp"], max_depth=spec["max_depth"], seed=6, walk_chunk=chunk)
+        img, _ = s.image()
+        assert st["error_bits"] == 0
+        if ref is None:
+            ref = (st, img)
+            continue
+        for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests", "shadow_facet_tests",
+                  "shadow_box_steps"):
+            assert st[k] == ref[0][k], (chunk, k)
+        assert rrmse(img, ref[1]) < 1e-12, chunk
+
+
+def test_walk_chunk_is_validated(require_gpu):
+    from math_b200 import ntrace
+
+    spec, s = _scene("n3_small")
+    with pytest.raises(ntrace.NtraceError) as e:
+        s.render(spec["spp"], walk_chunk=48)
+    assert e.value.code == ntrace.NT_EINVAL
+
+
 def test_batch_of_mixed_dimensions_matches_single_renders(require_gpu):
     from math_b200 import ntrace
 
@@ -70,7 +99,8 @@ def test_batch_rejects_repeated_scene(require_gpu):
 def test_autotune_picks_a_candidate_and_clears(require_gpu):
     spec, s = _scene("n4_small")
     tuned, ms = s.autotune(spec["spp"], max_depth=spec["max_depth"])
-    assert tuned["graph_iterations"] in (2, 4, 8)
+    assert tuned["graph_iterations"] in (2, 4, 8, 16)
+    assert tuned["walk_chunk"] in (32, 64, 128)
     assert tuned["pool_paths"] >= 256 and ms > 0
     img, spp = s.image()
     assert spp == 0 and not img.any()
