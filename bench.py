@@ -42,7 +42,7 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-CONFIGS = {"n3": "n3", "n4": "n4", "n5": "n5"}
+CONFIGS = {"n3": "n3", "n4": "n4", "n5": "n5", "batch": "batch"}
 def metric_name(n: int) -> str:
     return f"paths/s per n (n={n} plain tracer)"
 
@@ -375,6 +375,23 @@ def measure_denoise(scene, n: int) -> dict:
                                  "input_rmse": p["input_rmse"]} for p in r["denoised"]]}
 
 
+def run_batch(args) -> None:
+    """--config batch: the batched mixed workload (math_b200.batched): 64 seeded scenes of n = 3..6 in
+    one CUDA graph per pass (nt_render_batch), tuned per dimension by nt_autotune; wall clock around
+    each synchronous batch call; hull meshes cached under _build/meshes between runs."""
+    from math_b200 import batched
+
+    os.environ.setdefault("NTRACE_NO_BUILD", "1")
+    r = batched.run(count=64, seed=0, repeat=args.steps, cache=ROOT / "_build" / "meshes")
+    print(json.dumps({
+        "metric": "paths/s (batched mixed workload, n = 3..6)", "value": r["batch_paths_per_s"], "unit": "paths/s",
+        "n_gpus": 1, "steps": args.steps, "warmup": 1, "ms_per_step": 1000 * r["batch_seconds"],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": r["workload"]}, "sequential_paths_per_s": r["sequential_paths_per_s"],
+        "paths_per_pass": r["paths_per_pass"], "tuned": r["tuned"], "dims": r["dims"], "facets": r["facets"],
+        "screens": r["screens"]}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -390,10 +407,18 @@ def main() -> None:
     args.warmup = max(args.warmup, 3)
 
     if args.impl == "reference":
+        if args.config == "batch":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched mixed workload has no reference "
+                              "counterpart (the reference paints one scene per paint() call)"}))
+            return
         run_reference(args)
         return
 
     import torch
+
+    if args.config == "batch":
+        run_batch(args)
+        return
 
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

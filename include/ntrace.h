@@ -79,9 +79,11 @@ typedef struct nt_render_opts
                                    process renders them); 0: continue after the samples already accumulated
                                    (progressive passes).  The accumulator's sample count grows by the pass's
                                    samples either way. */
-        int walk_chunk;         /* tree-walk kernels: pooled facet tests whose records a warp stages in shared
-                                   memory at once, 32, 64 or 128; 0: the default for n (128 at n = 3, 64 at
-                                   n = 4 and 5, 32 at n = 6).  nt_autotune picks it. */
+        int walk_chunk;         /* tree-walk kernels: 1: facet records read straight from global memory, 32
+                                   pooled tests per round; 32, 64 or 128: that many pooled tests per warp
+                                   have their records staged in shared memory at once (cp.async); 0: the
+                                   default (1).  A tuning choice only: every variant makes the same
+                                   decisions.  nt_autotune picks it. */
 } nt_render_opts;
 
 typedef struct nt_stats
@@ -255,7 +257,7 @@ int nt_accum_clear(nt_scene* scene);
 int nt_render_batch(nt_scene* const* scenes, int count, const nt_render_opts* opts, nt_stats* stats);
 
 /* Times probe passes of `base` (its samples per pixel) over candidate path-pool sizes and iterations
- * per graph launch, then over the walk kernels' staging chunks (walk_chunk 32, 64, 128) at the best
+ * per graph launch, then over the walk kernels' variants (walk_chunk 1, 32, 64, 128) at the best
  * of those, and returns the fastest in *tuned (a copy of base with pool_paths, graph_iterations and
  * walk_chunk set) and its pass time in *best_ms (may be NULL).  The probe passes go to the scene's
  * accumulator, which is cleared afterwards. */

@@ -1295,13 +1295,14 @@ struct StageFit
         static constexpr int ROUNDS = FIT < 1 ? 1 : (FIT > 4 ? 4 : (FIT == 3 ? 2 : FIT));
 };
 
+// R = 0: no staging; the records are read straight from global memory, 32 tests per round.
 template <int N, int R = StageFit<N>::ROUNDS>
 struct Stage
 {
         static constexpr int REC_BYTES = Rec32<N>::F4 * 16;
-        static constexpr int ROUNDS = R;
+        static constexpr int ROUNDS = R > 0 ? R : 1;
         static constexpr int SLOTS = 32 * ROUNDS;
-        static constexpr int BYTES = (WALK_BLOCK / 32) * SLOTS * REC_BYTES;
+        static constexpr int BYTES = R > 0 ? (WALK_BLOCK / 32) * SLOTS * REC_BYTES : 0;
         static_assert(SLOTS <= POOL_SLOTS, "a chunk's outcomes must fit the warp's pool");
 };
 
@@ -1355,13 +1356,14 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                 return best;
         }
         PoolSlot* pool = warp_pool();
-        constexpr int R = RR;
+        constexpr bool STAGED = RR > 0;
+        constexpr int R = Stage<N, RR>::ROUNDS;
         constexpr int F4 = Rec32<N>::F4;
-        float4* const stage = stage_base() + (size_t)(threadIdx.x >> 5) * Stage<N, R>::SLOTS * F4;
+        float4* const stage = stage_base() + (size_t)(threadIdx.x >> 5) * Stage<N, RR>::SLOTS * F4;
         const Ray64Source<N> own_src{raw_org, raw_dir, raw};
-        for (int cb = 0; cb < total; cb += Stage<N, R>::SLOTS)
+        for (int cb = 0; cb < total; cb += Stage<N, RR>::SLOTS)
         {
-                const int ce = min(total, cb + Stage<N, R>::SLOTS);
+                const int ce = min(total, cb + Stage<N, RR>::SLOTS);
                 // the chunk's facet indices (independent loads), then their records into the staging
                 // slots (all copies in flight at once)
                 int own[R];
@@ -1386,21 +1388,24 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                         const int o_excl = __shfl_sync(full, excl, o);
                         fid[r] = (k < ce) ? __ldg(&M.leaf_idx[o_start + (k - o_excl)]) : -1;
                 }
-#pragma unroll
-                for (int r = 0; r < R; ++r)
+                if constexpr (STAGED)
                 {
-                        if (fid[r] >= 0)
-                        {
-                                const float4* src = M.rec32 + (size_t)fid[r] * F4;
-                                float4* dst = stage + (size_t)(32 * r + lane) * F4;
 #pragma unroll
-                                for (int q = 0; q < F4; ++q)
+                        for (int r = 0; r < R; ++r)
+                        {
+                                if (fid[r] >= 0)
                                 {
-                                        cp_async16(dst + q, src + q);
+                                        const float4* src = M.rec32 + (size_t)fid[r] * F4;
+                                        float4* dst = stage + (size_t)(32 * r + lane) * F4;
+#pragma unroll
+                                        for (int q = 0; q < F4; ++q)
+                                        {
+                                                cp_async16(dst + q, src + q);
+                                        }
                                 }
                         }
+                        cp_async_wait_all();
                 }
-                cp_async_wait_all();
 #pragma unroll
                 for (int r = 0; r < R; ++r)
                 {
@@ -1422,7 +1427,8 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                                 float t = -1.0f;
                                 double t64 = -1.0;
                                 int keep = -1;
-                                int res = facet_test32<N, true>(stage + (size_t)(32 * r + lane) * F4, rr, o_ao, &t);
+                                int res = STAGED ? facet_test32<N, true>(stage + (size_t)(32 * r + lane) * F4, rr, o_ao, &t)
+                                                 : facet_test32<N, false>(M.rec32 + (size_t)f * F4, rr, o_ao, &t);
                                 if (res == T_HIT)
                                 {
                                         keep = f;

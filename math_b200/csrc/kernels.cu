@@ -1146,6 +1146,12 @@ void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
         }
 }
 
+// The walk kernels' variant when the options leave it open: facet records read straight from global
+// memory (measured faster than staging them through shared memory on the configuration scenes, whose
+// leaves hold one or two facets per visit on average, so a warp's pooled list rarely fills a chunk).
+template <int N>
+constexpr int DEFAULT_WALK_ROUNDS = -1;
+
 // Resident blocks of every kernel of an iteration, and the dynamic shared memory of the walk kernels
 // (they stage facet records there, leaf_closest_warp): computed once per dimension, on the first call,
 // which the host makes before any capture (prepare_pass, nt_render_noalloc).
@@ -1156,12 +1162,14 @@ const LaunchSizes& Wavefront<N>::prepare()
                 LaunchSizes z;
                 z.extend_blocks = resident_blocks(k_extend<N>);
                 z.shadow_blocks = resident_blocks(k_shadow<N>);
-                z.extend_refill_blocks[0] = resident_blocks(k_extend_refill<N, 1>, Stage<N, 1>::BYTES);
-                z.extend_refill_blocks[1] = resident_blocks(k_extend_refill<N, 2>, Stage<N, 2>::BYTES);
-                z.extend_refill_blocks[2] = resident_blocks(k_extend_refill<N, 4>, Stage<N, 4>::BYTES);
-                z.shadow_refill_blocks[0] = resident_blocks(k_shadow_refill<N, 1>, Stage<N, 1>::BYTES);
-                z.shadow_refill_blocks[1] = resident_blocks(k_shadow_refill<N, 2>, Stage<N, 2>::BYTES);
-                z.shadow_refill_blocks[2] = resident_blocks(k_shadow_refill<N, 4>, Stage<N, 4>::BYTES);
+                z.extend_refill_blocks[0] = resident_blocks(k_extend_refill<N, 0>, Stage<N, 0>::BYTES);
+                z.extend_refill_blocks[1] = resident_blocks(k_extend_refill<N, 1>, Stage<N, 1>::BYTES);
+                z.extend_refill_blocks[2] = resident_blocks(k_extend_refill<N, 2>, Stage<N, 2>::BYTES);
+                z.extend_refill_blocks[3] = resident_blocks(k_extend_refill<N, 4>, Stage<N, 4>::BYTES);
+                z.shadow_refill_blocks[0] = resident_blocks(k_shadow_refill<N, 0>, Stage<N, 0>::BYTES);
+                z.shadow_refill_blocks[1] = resident_blocks(k_shadow_refill<N, 1>, Stage<N, 1>::BYTES);
+                z.shadow_refill_blocks[2] = resident_blocks(k_shadow_refill<N, 2>, Stage<N, 2>::BYTES);
+                z.shadow_refill_blocks[3] = resident_blocks(k_shadow_refill<N, 4>, Stage<N, 4>::BYTES);
                 z.stream_blocks = resident_blocks(k_shade<N>);
                 return z;
         }();
@@ -1176,9 +1184,10 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         const LaunchSizes& L = prepare();
         const long long extend_blocks = L.extend_blocks;
         const long long shadow_blocks = L.shadow_blocks;
-        // the walk kernels' staging chunk: 1, 2 or 4 rounds of 32 pooled tests per warp
-        const int rounds = S.walk_rounds > 0 ? S.walk_rounds : StageFit<N>::ROUNDS;
-        const int vi = rounds >= 4 ? 2 : (rounds >= 2 ? 1 : 0);
+        // the walk kernels' variant: records read directly (walk_rounds -1), or staged in chunks of 1, 2
+        // or 4 rounds of 32 pooled tests per warp
+        const int rounds = S.walk_rounds != 0 ? S.walk_rounds : DEFAULT_WALK_ROUNDS<N>;
+        const int vi = rounds < 0 ? 0 : (rounds >= 4 ? 3 : (rounds >= 2 ? 2 : 1));
         const long long extend_refill_blocks = L.extend_refill_blocks[vi];
         const long long shadow_refill_blocks = L.shadow_refill_blocks[vi];
         const long long stream_blocks = L.stream_blocks;
@@ -1211,9 +1220,13 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         {
                 if (vi == 0)
                 {
-                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, counters);
+                        k_extend_refill<N, 0><<<ext_grid, BLOCK, 0, st>>>(S, A, H, counters);
                 }
                 else if (vi == 1)
+                {
+                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, counters);
+                }
+                else if (vi == 2)
                 {
                         k_extend_refill<N, 2><<<ext_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, A, H, counters);
                 }
@@ -1239,9 +1252,13 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         {
                 if (vi == 0)
                 {
-                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, counters);
+                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, counters);
                 }
                 else if (vi == 1)
+                {
+                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, counters);
+                }
+                else if (vi == 2)
                 {
                         k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, counters);
                 }

@@ -1340,14 +1340,15 @@ struct PassJobN final : PassJob
         }
 };
 
-// The walk kernels' staging chunk in rounds of 32 tests (nt_render_opts.walk_chunk; 0: the default).
+// The walk kernels' variant (nt_render_opts.walk_chunk): -1 unstaged, else the staging chunk in rounds
+// of 32 tests; 0: the default.
 int walk_rounds(const nt_render_opts& o)
 {
-        if (o.walk_chunk != 0 && o.walk_chunk != 32 && o.walk_chunk != 64 && o.walk_chunk != 128)
+        if (o.walk_chunk != 0 && o.walk_chunk != 1 && o.walk_chunk != 32 && o.walk_chunk != 64 && o.walk_chunk != 128)
         {
-                fail(NT_EINVAL, "walk_chunk must be 0, 32, 64 or 128");
+                fail(NT_EINVAL, "walk_chunk must be 0, 1, 32, 64 or 128");
         }
-        return o.walk_chunk / 32;
+        return o.walk_chunk == 1 ? -1 : o.walk_chunk / 32;
 }
 
 // Where a pass's radiance goes when it is not the scene's per-pixel accumulator.
@@ -2582,7 +2583,7 @@ int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tun
                 }
                 // then the walk kernels' staging chunk at the best pool and iterations
                 const nt_render_opts at = best;
-                for (int chunk : {32, 64, 128})
+                for (int chunk : {1, 32, 64, 128})
                 {
                         nt_render_opts o = at;
                         o.walk_chunk = chunk;

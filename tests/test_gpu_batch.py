@@ -42,11 +42,12 @@ def test_graph_and_direct_iterations_trace_the_same_paths(require_gpu):
 
 @pytest.mark.parametrize("name", ["n3_small", "n4_small", "n5_small", "n6_small"])
 def test_walk_chunks_trace_the_same_paths(require_gpu, name):
-    """The walk kernels' staging chunk (32, 64 or 128 pooled facet tests per warp) is a tuning choice
-    only: every chunk makes the same decisions (same work counters, same image)."""
+    """The walk kernels' variant (records read directly, or staged in chunks of 32, 64 or 128 pooled
+    facet tests per warp) is a tuning choice only: every variant makes the same decisions (same work
+    counters, same image)."""
     spec, s = _scene(name)
     ref = None
-    for chunk in (32, 64, 128):
+    for chunk in (1, 32, 64, 128):
         s.clear()
         st = s.render(spec["spp"], max_depth=spec["max_depth"], seed=6, walk_chunk=chunk)
         img, _ = s.image()
@@ -100,7 +101,7 @@ def test_autotune_picks_a_candidate_and_clears(require_gpu):
     spec, s = _scene("n4_small")
     tuned, ms = s.autotune(spec["spp"], max_depth=spec["max_depth"])
     assert tuned["graph_iterations"] in (2, 4, 8, 16)
-    assert tuned["walk_chunk"] in (32, 64, 128)
+    assert tuned["walk_chunk"] in (1, 32, 64, 128)
     assert tuned["pool_paths"] >= 256 and ms > 0
     img, spp = s.image()
     assert spp == 0 and not img.any()
