@@ -59,7 +59,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
     BUILD_DIR.mkdir(parents=True, exist_ok=True)
     cu_obj = BUILD_DIR / "kernels.o"
     cpp_obj = BUILD_DIR / "scene.o"
-    common = ["-std=c++17", "-I", str(INCLUDE), "-I", str(CSRC)]
+    # NTRACE_DEFINES: extra -D options for the kernels (build-time tuning, e.g. -DNT_WALK_MIN_BLOCKS=3)
+    common = ["-std=c++17", "-I", str(INCLUDE), "-I", str(CSRC)] + os.environ.get("NTRACE_DEFINES", "").split()
     if force or _stale(cu_obj, [cu] + headers):
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC,-ffp-contract=off", *common,
                "-c", str(cu), "-o", str(cu_obj)]

@@ -744,14 +744,15 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
         bool b64 = false;
         for (int q = 0; q < leaf.y; ++q)
         {
-                int f = __ldg(&M.leaf_idx[leaf.x + q]);
                 ++ws->facet_tests;
                 float t;
-                int res = facet_test32<N>(M.rec32 + (size_t)f * Rec32<N>::F4, ray, ao, &t);
+                int res = facet_test32<N>(M.leaf_rec32 + (size_t)(leaf.x + q) * Rec32<N>::F4, ray, ao, &t);
                 if (res == T_MISS)
                 {
                         continue;
                 }
+                // the facet's index only for the tests that did not miss
+                const int f = __ldg(&M.leaf_idx[leaf.x + q]);
                 double t64 = 0;
                 bool is64 = false;
                 if (res == T_UNSURE)
@@ -1364,10 +1365,11 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
         for (int cb = 0; cb < total; cb += Stage<N, RR>::SLOTS)
         {
                 const int ce = min(total, cb + Stage<N, RR>::SLOTS);
-                // the chunk's facet indices (independent loads), then their records into the staging
-                // slots (all copies in flight at once)
+                // the chunk's entries (positions in the leaf lists, whose records lie in that order in
+                // leaf_rec32), then, staged, their records into the staging slots (all copies in flight
+                // at once); a facet's index is read only for the tests that do not miss
                 int own[R];
-                int fid[R];
+                int pos[R];
 #pragma unroll
                 for (int r = 0; r < R; ++r)
                 {
@@ -1386,16 +1388,16 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                         own[r] = o;
                         const int o_start = __shfl_sync(full, start, o);
                         const int o_excl = __shfl_sync(full, excl, o);
-                        fid[r] = (k < ce) ? __ldg(&M.leaf_idx[o_start + (k - o_excl)]) : -1;
+                        pos[r] = (k < ce) ? o_start + (k - o_excl) : -1;
                 }
                 if constexpr (STAGED)
                 {
 #pragma unroll
                         for (int r = 0; r < R; ++r)
                         {
-                                if (fid[r] >= 0)
+                                if (pos[r] >= 0)
                                 {
-                                        const float4* src = M.rec32 + (size_t)fid[r] * F4;
+                                        const float4* src = M.leaf_rec32 + (size_t)pos[r] * F4;
                                         float4* dst = stage + (size_t)(32 * r + lane) * F4;
 #pragma unroll
                                         for (int q = 0; q < F4; ++q)
@@ -1422,13 +1424,13 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                         const long long o_raw = raw_org ? __shfl_sync(full, raw, o) : 0;
                         if (k < ce)
                         {
-                                const int f = fid[r];
                                 ++ws->facet_tests;
                                 float t = -1.0f;
                                 double t64 = -1.0;
                                 int keep = -1;
                                 int res = STAGED ? facet_test32<N, true>(stage + (size_t)(32 * r + lane) * F4, rr, o_ao, &t)
-                                                 : facet_test32<N, false>(M.rec32 + (size_t)f * F4, rr, o_ao, &t);
+                                                 : facet_test32<N, false>(M.leaf_rec32 + (size_t)pos[r] * F4, rr, o_ao, &t);
+                                const int f = res != T_MISS ? __ldg(&M.leaf_idx[pos[r]]) : -1;
                                 if (res == T_HIT)
                                 {
                                         keep = f;

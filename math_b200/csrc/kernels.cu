@@ -1450,6 +1450,30 @@ cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, floa
         return cudaGetLastError();
 }
 
+// out[j] = rec[idx[j]] for records of f4 float4s (the leaves' records in leaf-list order)
+__global__ void k_gather_records(const float4* __restrict__ rec, const int* __restrict__ idx, long long count, int f4,
+                                 float4* __restrict__ out)
+{
+        const long long total = count * f4;
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x)
+        {
+                const long long j = i / f4;
+                const int q = (int)(i - j * f4);
+                out[i] = __ldg(rec + (size_t)__ldg(idx + j) * f4 + q);
+        }
+}
+
+cudaError_t launch_gather_records(const float4* rec, const int* idx, long long count, int f4, float4* out,
+                                  cudaStream_t st)
+{
+        if (count > 0)
+        {
+                const unsigned g = (unsigned)std::min<long long>((count * f4 + BLOCK - 1) / BLOCK, 148LL * 64);
+                k_gather_records<<<g, BLOCK, 0, st>>>(rec, idx, count, f4, out);
+        }
+        return cudaGetLastError();
+}
+
 cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, float* mean, float* var, cudaStream_t st)
 {
         const unsigned g = (unsigned)std::min<long long>((npix * 3 + BLOCK - 1) / BLOCK, 148LL * 32);

@@ -95,6 +95,10 @@ template <int N>
 cudaError_t launch_aux(const DevScene<N>& S, long long npix, float* normal, float* depth, cudaStream_t st);
 cudaError_t launch_moments_reduce(long long npix, int spp, const double* rad, float* mean, float* var, cudaStream_t st);
 
+// out[j] = rec[idx[j]] for count records of f4 float4s each (the leaves' records in leaf-list order).
+cudaError_t launch_gather_records(const float4* rec, const int* idx, long long count, int f4, float4* out,
+                                  cudaStream_t st);
+
 // Mean colour per pixel (floats) from the per-pixel sums.
 cudaError_t launch_mean(long long n3, const double* sums, long long samples, float* out, cudaStream_t st);
 

@@ -237,6 +237,7 @@ struct MeshHost
         double build_seconds = 0;
         std::vector<int32_t> ntype;  // per facet: NormalType and reversed-vertex bits (MeshDev::ntype)
         DevBuf d_rec32, d_rec64, d_nodes, d_idx;
+        DevBuf d_leafrec;  // rec32 gathered in leaf-list order (made on the device from d_rec32, d_idx)
         DevBuf d_normals, d_fnormals, d_ntype;
         // device staging copy of the four arrays (nt_scene_upload_begin / _commit)
         DevBuf d_stage;
@@ -259,7 +260,8 @@ struct MeshHost
                   dist(o.dist), vmin(std::move(o.vmin)), vmax(std::move(o.vmax)), leaf_count(o.leaf_count),
                   degenerate(o.degenerate), build_seconds(o.build_seconds), ntype(std::move(o.ntype)),
                   d_rec32(std::move(o.d_rec32)), d_rec64(std::move(o.d_rec64)), d_nodes(std::move(o.d_nodes)),
-                  d_idx(std::move(o.d_idx)), d_normals(std::move(o.d_normals)), d_fnormals(std::move(o.d_fnormals)),
+                  d_idx(std::move(o.d_idx)), d_leafrec(std::move(o.d_leafrec)), d_normals(std::move(o.d_normals)),
+                  d_fnormals(std::move(o.d_fnormals)),
                   d_ntype(std::move(o.d_ntype)), d_stage(std::move(o.d_stage)),
                   pinned(o.pinned), pinned_bytes(o.pinned_bytes), ready(o.ready), uploaded(o.uploaded)
         {
@@ -937,6 +939,27 @@ void copy_obj(ObjDev* o, int kind, int index, const nt_surface& s)
         o->light_source = s.light_source;
 }
 
+// FP32 record size in float4s at dimension n (Rec32<n>::F4).
+int rec32_f4(int n)
+{
+        return (n * n + n + 2 + 3) / 4;
+}
+
+// The leaves' records in leaf-list order, gathered on the device from the uploaded record and index
+// arrays (after every upload of those, on the scene's stream).
+void gather_leaf_records(MeshHost& m, int n, cudaStream_t st)
+{
+        const long long count = (long long)(m.d_idx.bytes / sizeof(int32_t));
+        const size_t bytes = std::max<size_t>((size_t)count * rec32_f4(n) * 16, 16);
+        if (m.d_leafrec.bytes != bytes)
+        {
+                m.d_leafrec.alloc(bytes);
+        }
+        check_cuda(launch_gather_records(m.d_rec32.as<float4>(), m.d_idx.as<int>(), count, rec32_f4(n),
+                                         m.d_leafrec.as<float4>(), st),
+                   "gather leaf records");
+}
+
 template <int N>
 MeshDev<N> mesh_dev(const MeshHost& m)
 {
@@ -945,6 +968,7 @@ MeshDev<N> mesh_dev(const MeshHost& m)
         d.rec64 = m.d_rec64.as<double>();
         d.nodes = m.d_nodes.as<int2>();
         d.leaf_idx = m.d_idx.as<int>();
+        d.leaf_rec32 = m.d_leafrec.as<float4>();
         d.vnormals = m.ntype.empty() ? nullptr : m.d_normals.as<float>();
         d.fnormals = m.ntype.empty() ? nullptr : m.d_fnormals.as<int>();
         d.ntype = m.ntype.empty() ? nullptr : m.d_ntype.as<int>();
@@ -1021,6 +1045,7 @@ void build_scene(nt_scene* s, unsigned threads, bool host_only, bool tree_on_gpu
                         m.d_rec64.upload(m.rec64, s->stream);
                         m.d_nodes.upload(m.nodes, s->stream);
                         m.d_idx.upload(m.leaf_idx, s->stream);
+                        gather_leaf_records(m, N, s->stream);
                         if (!m.ntype.empty())
                         {
                                 m.d_normals.upload(m.normals, s->stream);
@@ -2138,7 +2163,8 @@ int nt_scene_mesh_info(nt_scene* scene, int mesh_index, nt_mesh_info* info)
                 info->distance_from_facet = m.dist;
                 info->degenerate_facets = m.degenerate;
                 info->build_seconds = m.build_seconds;
-                info->device_bytes = (int64_t)(m.d_rec32.bytes + m.d_rec64.bytes + m.d_nodes.bytes + m.d_idx.bytes);
+                info->device_bytes =
+                        (int64_t)(m.d_rec32.bytes + m.d_rec64.bytes + m.d_nodes.bytes + m.d_idx.bytes + m.d_leafrec.bytes);
         });
 }
 
@@ -2198,6 +2224,7 @@ int nt_scene_upload(nt_scene* scene, int64_t* bytes)
                                 p += b->bytes;
                                 total += (int64_t)b->bytes;
                         }
+                        gather_leaf_records(m, scene->n, scene->stream);
                 }
                 check_cuda(cudaStreamSynchronize(scene->stream), "upload sync");
                 if (bytes)
@@ -2278,6 +2305,11 @@ int nt_scene_upload_commit(nt_scene* scene)
                         }
                 }
                 check_cuda(cudaEventRecord(scene->consumed, scene->stream), "record");
+                // the leaf-ordered records are made from the live arrays, after the staging buffer is free
+                for (auto& m : scene->meshes)
+                {
+                        gather_leaf_records(m, scene->n, scene->stream);
+                }
                 scene->consumed_recorded = true;
                 scene->upload_staged = false;
         });
