@@ -316,7 +316,7 @@ def measure_plain(scene, spec: dict, args, steps: int, rank: int, world: int, lo
     return out
 
 
-def roofline(n: int, timed: dict, name: str, pool_paths: int) -> dict:
+def roofline(n: int, timed: dict, name: str, pool_paths: int, probes: dict | None = None) -> dict:
     """Roofline of the dominant walk kernel (the one with the larger device time) from the timing pass:
     algorithmic bytes per launch (the reference algorithm's work counters, algorithmic_work) over the
     launch's CUDA-event time, against the measured HBM copy peak."""
@@ -333,24 +333,41 @@ def roofline(n: int, timed: dict, name: str, pool_paths: int) -> dict:
     # DRAM bytes per launch from an ncu capture (profiles/traffic.json), scaled by the algorithmic bytes
     # of this run's launches over those of the captured ones when the pool size differs (a launch's
     # traffic grows with the rays it processes)
-    traffic = None
+    traffic = l2_traffic = None
     tf = ROOT / "profiles" / "traffic.json"
     if tf.exists():
         try:
             t = json.loads(tf.read_text())
-            traffic = t.get(f"{name}_{dom}_bytes_per_launch")
             alg = t.get(f"{name}_{dom}_algorithmic_bytes_per_launch")
-            if traffic is not None and t.get("pool_paths") != pool_paths:
-                traffic = traffic * walks[dom]["bytes"] / alg if alg else None
+            scale = walks[dom]["bytes"] / alg if alg else None
+            traffic = t.get(f"{name}_{dom}_bytes_per_launch")
+            l2_traffic = t.get(f"{name}_{dom}_l2_bytes_per_launch")
+            if scale is not None:
+                traffic = traffic * scale if traffic is not None else None
+                l2_traffic = l2_traffic * scale if l2_traffic is not None else None
         except Exception:
-            traffic = None
+            traffic = l2_traffic = None
     achieved = walks[dom]["achieved"]
-    return {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
-            "kernel": "k_shadow_refill" if dom == "shadow" else "k_extend_refill",
-            "peak_source": peaks["source"], "algorithmic_bytes_per_launch": walks[dom]["bytes"],
-            "algorithmic_flops_per_launch": walks[dom]["flops"], "launch_ms": walks[dom]["launch_ms"],
-            "walk_algorithmic_gbs": {k: w["achieved"] for k, w in walks.items()}}
+    launch_s = walks[dom]["launch_ms"] / 1000.0
+    out = {"bound": "hbm", "achieved": achieved, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": achieved / peaks["hbm_gbs"], "traffic": traffic,
+           "kernel": "k_shadow_refill" if dom == "shadow" else "k_extend_refill",
+           "peak_source": peaks["source"], "algorithmic_bytes_per_launch": walks[dom]["bytes"],
+           "algorithmic_flops_per_launch": walks[dom]["flops"], "launch_ms": walks[dom]["launch_ms"],
+           "walk_algorithmic_gbs": {k: w["achieved"] for k, w in walks.items()}}
+    if probes:
+        # the other two ceilings of the walk: its L2 traffic (the ncu capture's L2 sectors per launch,
+        # scaled like the DRAM traffic) against the L2 read rate, and its algorithmic FP32 flops against
+        # the FMA rate, both peaks measured by the library's probe kernels (nt_probe_peaks)
+        if l2_traffic is not None and launch_s > 0:
+            a = l2_traffic / launch_s / 1e9
+            out["l2"] = {"achieved": a, "peak": probes["l2_read_gbs"], "unit": "GB/s",
+                         "frac": a / probes["l2_read_gbs"], "traffic": l2_traffic, "peak_source": "nt_probe_peaks"}
+        if launch_s > 0:
+            a = walks[dom]["flops"] / launch_s / 1e12
+            out["fp32"] = {"achieved": a, "peak": probes["fp32_fma_tflops"], "unit": "TFLOP/s",
+                           "frac": a / probes["fp32_fma_tflops"], "peak_source": "nt_probe_peaks"}
+    return out
 
 
 def measure_denoise(scene, n: int) -> dict:
@@ -451,6 +468,9 @@ def main() -> None:
     spec = scenes.config(args.config)
     n = spec["n"]
     scene = scenes.build_scene(spec, tree_on_gpu=True)
+    from math_b200 import ntrace
+
+    probes = ntrace.probe_peaks()
     m = measure_plain(scene, spec, args, args.steps, rank, world, local, dist)
     timed, tuned = m["timed"], m["tuned"]
 
@@ -464,9 +484,10 @@ def main() -> None:
                    "walk_chunk": tuned["walk_chunk"], "tuned_by": "nt_autotune"},
         "e2e": m["e2e"],
         "gpu_launches": m["launches"],
-        "roofline": roofline(n, timed, args.config, tuned["pool_paths"]),
-        "kernels_ms_per_frame": {"raygen": timed["raygen_ms"], "extend": timed["extend_ms"], "shade": timed["shade_ms"],
-                                 "shadow": timed["shadow_ms"]},
+        "roofline": roofline(n, timed, args.config, tuned["pool_paths"], probes),
+        "probed_peaks": probes,
+        "kernels_ms_per_frame": {"raygen": timed["raygen_ms"], "plan": timed["plan_ms"], "extend": timed["extend_ms"],
+                                 "shade": timed["shade_ms"], "shadow": timed["shadow_ms"]},
         "counters_per_frame": {k: timed[k] for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests",
                                                      "descent_levels", "shadow_facet_tests", "shadow_box_steps",
                                                      "shadow_retests", "shadow_descent_levels")},
@@ -497,9 +518,9 @@ def main() -> None:
                         "tuning": {"pool_paths": mm["tuned"]["pool_paths"],
                                    "graph_iterations": mm["tuned"]["graph_iterations"],
                                    "walk_chunk": mm["tuned"]["walk_chunk"]},
-                        "roofline": roofline(sp["n"], mm["timed"], c, mm["tuned"]["pool_paths"]),
-                        "kernels_ms_per_frame": {kk: mm["timed"][kk + "_ms"] for kk in ("raygen", "extend", "shade",
-                                                                                        "shadow")},
+                        "roofline": roofline(sp["n"], mm["timed"], c, mm["tuned"]["pool_paths"], probes),
+                        "kernels_ms_per_frame": {kk: mm["timed"][kk + "_ms"] for kk in ("raygen", "plan", "extend",
+                                                                                        "shade", "shadow")},
                         "clocks": mm["clocks"], "device_errors": mm["device_errors"]}
             try:
                 denoise_res[c] = measure_denoise(sc, sp["n"])

@@ -111,6 +111,8 @@ typedef struct nt_stats
         int64_t shadow_retests;
         int64_t shadow_descent_levels;
         int64_t iterations;       /* wavefront iterations that had work */
+        double plan_ms;           /* device time of the plan-and-compact kernels of one-mesh scenes (timing = 1):
+                                     they finish the rays that need no tree walk and list the others */
 } nt_stats;
 
 typedef struct nt_mesh_info
@@ -340,6 +342,20 @@ int nt_convex_hull(int n, const float* points, int64_t count, nt_hull** out);
 int64_t nt_hull_facet_count(nt_hull* hull);
 int nt_hull_facets(nt_hull* hull, int32_t* facets);
 int nt_hull_destroy(nt_hull* hull);
+
+/* ---- peaks of this GPU for the rooflines (no counterpart in the reference) ---- */
+
+typedef struct nt_peaks
+{
+        double l2_read_gbs;      /* L2 read bandwidth: 16-byte loads bypassing L1 over a 32 MiB resident buffer */
+        double fp32_fma_tflops;  /* FP32 FMA rate: eight independent fmaf chains per thread, 2 flops per FMA */
+        double l2_ms;            /* the timed launches */
+        double fma_ms;
+} nt_peaks;
+
+/* Measures the two ceilings of the tree-walk kernels besides the HBM copy rate with kernels of this
+ * library, timed with CUDA events on the current device (allocates and frees 32 MiB). */
+int nt_probe_peaks(nt_peaks* out);
 
 /* ---- misc ---- */
 

@@ -83,6 +83,13 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
+    probes = CSRC / "probes.cu"
+    probes_obj = BUILD_DIR / "probes.o"
+    if force or _stale(probes_obj, [probes, INCLUDE / "ntrace.h"]):
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-Xcompiler", "-fPIC", *common, "-c", str(probes), "-o", str(probes_obj)]
+        if verbose:
+            print(" ".join(cmd))
+        _run(cmd)
     denoise = CSRC / "denoise.cu"
     denoise_obj = BUILD_DIR / "denoise.o"
     if force or _stale(denoise_obj, [denoise] + headers + [INCLUDE / "ntrace_denoise.h"]):
@@ -117,9 +124,10 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if verbose:
             print(" ".join(cmd))
         _run(cmd)
-    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, denoise_obj, objload_obj, tree_obj, hull_obj]):
+    if force or _stale(LIB, [cu_obj, cpp_obj, noalloc_obj, probes_obj, denoise_obj, objload_obj, tree_obj, hull_obj]):
         cmd = [nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(LIB), str(cu_obj), str(cpp_obj),
-               str(noalloc_obj), str(denoise_obj), str(objload_obj), str(tree_obj), str(hull_obj), "-Xlinker",
+               str(noalloc_obj), str(probes_obj), str(denoise_obj), str(objload_obj), str(tree_obj), str(hull_obj),
+               "-Xlinker",
                "--no-undefined", "-lpthread"]
         if verbose:
             print(" ".join(cmd))

@@ -700,13 +700,142 @@ __device__ __forceinline__ long long lane_refill(bool idle, unsigned long long* 
         return j < count ? j : -1;
 }
 
-// Extension rays of a scene with one mesh: closest_plan at fetch, then one leaf per iteration.
+// Appends this lane's queue index to a walk list when `walk` (one atomic per warp; the lanes of a warp
+// keep their order).  Every lane of the warp calls it.
+__device__ __forceinline__ void list_append(bool walk, long long i, int* list, unsigned long long* count)
+{
+        const unsigned m = __ballot_sync(0xffffffffu, walk);
+        if (!m)
+        {
+                return;
+        }
+        const int lane = threadIdx.x & 31;
+        const int leader = __ffs(m) - 1;
+        unsigned long long base = 0;
+        if (lane == leader)
+        {
+                base = atomicAdd(count, (unsigned long long)__popc(m));
+        }
+        base = __shfl_sync(0xffffffffu, base, leader);
+        if (walk)
+        {
+                list[base + __popc(m & lanemask_lt())] = (int)i;
+        }
+}
+
+// Extension rays of a scene with one mesh, first pass: every ray's objects (closest_plan); the rays
+// that need no tree walk are finished here (their hit record written), the others are compacted into
+// the walk list for k_extend_refill, so that its lanes only ever hold rays that walk.
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H,
+                                                       int* __restrict__ list, unsigned long long* counters)
+{
+        const long long count = (long long)counters[C_Q_ACTIVE];
+        const int lane = threadIdx.x & 31;
+        const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+        long long rays = 0;
+        for (long long w0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; w0 < count;
+             w0 += warps * 32)
+        {
+                const long long i = w0 + lane;
+                bool walk = false;
+                if (i < count)
+                {
+                        ++rays;
+                        Ray<N> r;
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                r.org[k] = A.at(k, i);
+                                r.dir[k] = A.at(N + k, i);
+                        }
+                        ClosestPlan plan;
+                        closest_plan<N>(S, r, &plan);
+                        walk = plan.walk;
+                        if (!walk)
+                        {
+                                if (plan.pre_obj >= 0)
+                                {
+                                        H.t[i] = plan.pre_t;
+                                        H.obj[i] = plan.pre_obj;
+                                        H.facet[i] = -1;
+                                }
+                                else
+                                {
+                                        H.obj[i] = -1;
+                                }
+                        }
+                }
+                list_append(walk, i, list, counters + C_WALK_EXT);
+        }
+        warp_add(counters + C_RAYS, rays);
+}
+
+// Shadow rays of a scene with one mesh, first pass: a non-mesh object nearer than the light occludes
+// at once; a ray whose mesh root box starts beyond the light (or is missed) reaches the light and adds
+// its contribution here; the rest are compacted into the walk list for k_shadow_refill.
+template <int N>
+__global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ,
+                                                       double* accum, int* __restrict__ list,
+                                                       unsigned long long* counters)
+{
+        const long long count = (long long)counters[C_SHADOW];
+        const int lane = threadIdx.x & 31;
+        const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
+        long long rays = 0;
+        for (long long w0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; w0 < count;
+             w0 += warps * 32)
+        {
+                const long long j = w0 + lane;
+                bool walk = false;
+                if (j < count)
+                {
+                        ++rays;
+                        Ray<N> r;
+#pragma unroll
+                        for (int k = 0; k < N; ++k)
+                        {
+                                r.org[k] = SQ.at(k, j);
+                                r.dir[k] = SQ.at(N + k, j);
+                        }
+                        const float dj = SQ.at(2 * N, j);
+                        bool occluded = false;
+                        for (int o = 0; o < S.nobj; ++o)
+                        {
+                                float a;
+                                if (!obj_approx<N>(S, o, r, &a) || !(a < dj))
+                                {
+                                        continue;
+                                }
+                                if (S.obj[o].kind == OBJ_MESH)
+                                {
+                                        walk = true;
+                                }
+                                else
+                                {
+                                        occluded = true;
+                                }
+                        }
+                        walk = walk && !occluded;
+                        if (!occluded && !walk)
+                        {
+                                accumulate(accum, SQ.pix[j], SQ.at(2 * N + 1, j), SQ.at(2 * N + 2, j), SQ.at(2 * N + 3, j));
+                        }
+                }
+                list_append(walk, j, list, counters + C_WALK_SH);
+        }
+        warp_add(counters + C_SHADOW_RAYS, rays);
+}
+
+// Extension rays of a scene with one mesh that walk the tree (the plan kernel's list): closest_plan
+// again at fetch (cheap: slab tests), then one leaf per iteration.
 // R: rounds of 32 pooled facet tests staged per warp chunk (Stage<N, R>).
 template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
-        k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, unsigned long long* counters)
+        k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, const int* __restrict__ list,
+                        unsigned long long* counters)
 {
-        const long long count = (long long)counters[C_Q_ACTIVE];
+        const long long count = (long long)counters[C_WALK_EXT];
         const MeshDev<N>& M = S.mesh[0];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
@@ -717,14 +846,14 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         ClosestPlan plan;
         while (true)
         {
-                // fill: rays that need no walk are finished here, so keep taking rays (a bounded number
-                // of rounds) until every lane holds one that does
+                // fill: every listed ray walks (the plan kernel finished the others), so one round fills
+                // every idle lane while rays remain
                 for (int round = 0; round < FILL_ROUNDS; ++round)
                 {
-                        long long j = lane_refill(i < 0, counters + C_WORK_EXT, count, &exhausted);
-                        if (j >= 0)
+                        const long long q = lane_refill(i < 0, counters + C_WORK_EXT, count, &exhausted);
+                        if (q >= 0)
                         {
-                                ++rays;
+                                const long long j = list[q];
                                 Ray<N> r;
 #pragma unroll
                                 for (int k = 0; k < N; ++k)
@@ -792,9 +921,10 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
 // otherwise the mesh is walked (up to the light's distance) when its root box starts before the light.
 template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
-        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, unsigned long long* counters)
+        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, const int* __restrict__ list,
+                        unsigned long long* counters)
 {
-        const long long count = (long long)counters[C_SHADOW];
+        const long long count = (long long)counters[C_WALK_SH];
         const MeshDev<N>& M = S.mesh[0];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
@@ -807,10 +937,11 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         {
                 for (int round = 0; round < FILL_ROUNDS; ++round)
                 {
-                        long long j = lane_refill(i < 0, counters + C_WORK_SH, count, &exhausted);
-                        if (j >= 0)
+                        const long long q = lane_refill(i < 0, counters + C_WORK_SH, count, &exhausted);
+                        if (q >= 0)
                         {
-                                ++rays;
+                                // a listed ray walks (k_plan_shadow); its mesh's entry distance again here
+                                const long long j = list[q];
                                 Ray<N> r;
 #pragma unroll
                                 for (int k = 0; k < N; ++k)
@@ -1016,6 +1147,8 @@ __global__ void k_iter_begin(unsigned long long* c, long long total, long long Q
         c[C_ACTIVE_OUT] = 0;
         c[C_SHADOW] = 0;
         c[C_SMOOTH] = 0;
+        c[C_WALK_EXT] = 0;
+        c[C_WALK_SH] = 0;
         if (active + fresh > 0)
         {
                 c[C_ITERS] += 1;
@@ -1107,8 +1240,9 @@ size_t Wavefront<N>::bytes_for(long long Q, int lights, bool smooth)
         size_t per_path = sizeof(float) * (2 * N + 4) * 2  // path state A and B
                           + sizeof(uint32_t) * 2 * 2 + sizeof(int) * 2
                           + sizeof(float) + sizeof(int) * 2  // hit record
-                          + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights * (smooth ? 2 : 1);  // shadow queues
-        return per_path * (size_t)Q + 18 * 256;
+                          + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights * (smooth ? 2 : 1)  // shadow queues
+                          + sizeof(int) * (1 + (size_t)lights);  // walk lists
+        return per_path * (size_t)Q + 20 * 256;
 }
 
 template <int N>
@@ -1134,6 +1268,8 @@ void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
         hit_facet = (int*)take(sizeof(int) * Q);
         sq_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
         sq_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
+        walk_ext = (int*)take(sizeof(int) * Q);
+        walk_sh = (int*)take(sizeof(int) * Q * lights);
         if (smooth)
         {
                 sm_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
@@ -1218,21 +1354,30 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (one_mesh)
         {
+                // rays that need no walk are finished by the plan kernel; the walk kernel takes the rest
+                k_plan_extend<N><<<str_grid, BLOCK, 0, st>>>(S, A, H, walk_ext, counters);
+        }
+        if (ev)
+        {
+                cudaEventRecord(ev[2], st);
+        }
+        if (one_mesh)
+        {
                 if (vi == 0)
                 {
-                        k_extend_refill<N, 0><<<ext_grid, BLOCK, 0, st>>>(S, A, H, counters);
+                        k_extend_refill<N, 0><<<ext_grid, BLOCK, 0, st>>>(S, A, H, walk_ext, counters);
                 }
                 else if (vi == 1)
                 {
-                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, counters);
+                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, walk_ext, counters);
                 }
                 else if (vi == 2)
                 {
-                        k_extend_refill<N, 2><<<ext_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, A, H, counters);
+                        k_extend_refill<N, 2><<<ext_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, A, H, walk_ext, counters);
                 }
                 else
                 {
-                        k_extend_refill<N, 4><<<ext_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, A, H, counters);
+                        k_extend_refill<N, 4><<<ext_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, A, H, walk_ext, counters);
                 }
         }
         else
@@ -1241,30 +1386,38 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (ev)
         {
-                cudaEventRecord(ev[2], st);
+                cudaEventRecord(ev[3], st);
         }
         k_shade<N><<<str_grid, BLOCK, 0, st>>>(S, P, A, H, B, SQ, SM, accum, counters);
         if (ev)
         {
-                cudaEventRecord(ev[3], st);
+                cudaEventRecord(ev[4], st);
+        }
+        if (one_mesh)
+        {
+                k_plan_shadow<N><<<str_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, counters);
+        }
+        if (ev)
+        {
+                cudaEventRecord(ev[5], st);
         }
         if (one_mesh)
         {
                 if (vi == 0)
                 {
-                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, counters);
+                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, counters);
                 }
                 else if (vi == 1)
                 {
-                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, counters);
+                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, walk_sh, counters);
                 }
                 else if (vi == 2)
                 {
-                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, counters);
+                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, walk_sh, counters);
                 }
                 else
                 {
-                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, counters);
+                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, walk_sh, counters);
                 }
         }
         else
@@ -1277,12 +1430,12 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (ev)
         {
-                cudaEventRecord(ev[4], st);
+                cudaEventRecord(ev[6], st);
         }
         k_iter_end<<<1, 1, 0, st>>>(counters, total_paths);
         if (times)
         {
-                times->launches += iteration_launches(smooth);
+                times->launches += iteration_launches(smooth, one_mesh);
                 times->extend_launches += 1;
                 times->shadow_launches += 1;
         }
@@ -1337,7 +1490,7 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                         e = cudaSuccess;
                 }
         }
-        cudaEvent_t ev[6];
+        cudaEvent_t ev[8];
         if (timing)
         {
                 for (auto& v : ev)
@@ -1359,16 +1512,20 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                         {
                                 enqueue_iteration(S, P, accum, counters, total_paths, parity, st, times, ev);
                                 parity ^= 1;
-                                cudaEventRecord(ev[5], st);
-                                cudaEventSynchronize(ev[5]);
+                                cudaEventRecord(ev[7], st);
+                                cudaEventSynchronize(ev[7]);
                                 float ms;
                                 cudaEventElapsedTime(&ms, ev[0], ev[1]);
                                 times->raygen_ms += ms;
                                 cudaEventElapsedTime(&ms, ev[1], ev[2]);
-                                times->extend_ms += ms;
+                                times->plan_ms += ms;
                                 cudaEventElapsedTime(&ms, ev[2], ev[3]);
-                                times->shade_ms += ms;
+                                times->extend_ms += ms;
                                 cudaEventElapsedTime(&ms, ev[3], ev[4]);
+                                times->shade_ms += ms;
+                                cudaEventElapsedTime(&ms, ev[4], ev[5]);
+                                times->plan_ms += ms;
+                                cudaEventElapsedTime(&ms, ev[5], ev[6]);
                                 times->shadow_ms += ms;
                         }
                 }
@@ -1379,7 +1536,7 @@ cudaError_t Wavefront<N>::run(const DevScene<N>& S, PassDev P, double* accum, un
                         {
                                 break;
                         }
-                        times->launches += (long long)per_replay * iteration_launches(smooth);
+                        times->launches += (long long)per_replay * iteration_launches(smooth, S.nmesh == 1);
                         times->extend_launches += per_replay;
                         times->shadow_launches += per_replay;
                 }

@@ -17,6 +17,7 @@ struct KernelTimes
         double extend_ms = 0;
         double shade_ms = 0;
         double shadow_ms = 0;
+        double plan_ms = 0;  // the plan-and-compact kernels of one-mesh scenes
         long long launches = 0;
         long long extend_launches = 0;
         long long shadow_launches = 0;
@@ -54,6 +55,9 @@ struct Wavefront
         int* hit_facet = nullptr;
         float* sq_f = nullptr;
         uint32_t* sq_pix = nullptr;
+        // one-mesh scenes: queue indices of the extension and shadow rays that walk the tree
+        int* walk_ext = nullptr;
+        int* walk_sh = nullptr;
         // smooth-normal shadow queue (only when some mesh has vertex normals and smooth_normal is set)
         float* sm_f = nullptr;
         uint32_t* sm_pix = nullptr;
@@ -74,13 +78,13 @@ struct Wavefront
 
         // One wavefront iteration on stream st (k_iter_begin .. k_iter_end; the queue sizes live in
         // counters, so nothing waits for the host).  parity selects which double-buffered queue is
-        // current; ev (6 events, optional) are recorded around the kernel kinds.  Capturable.
+        // current; ev (8 events, optional) are recorded around the kernel kinds.  Capturable.
         void enqueue_iteration(const DevScene<N>& S, const PassDev& P, double* accum, unsigned long long* counters,
                                long long total_paths, int parity, cudaStream_t st, KernelTimes* times,
                                cudaEvent_t* ev) const;
-        static int iteration_launches(bool smooth)
+        static int iteration_launches(bool smooth, bool one_mesh)
         {
-                return 6 + (smooth ? 1 : 0);
+                return 6 + (smooth ? 1 : 0) + (one_mesh ? 2 : 0);
         }
 
         // The iteration kernels' attributes (dynamic shared memory of the walk kernels) and grid sizes,

@@ -1338,6 +1338,7 @@ struct PassJob
         long long spp_eff = 0;
         bool smooth = false;
         bool counts_samples = true;  // the pass adds to the scene's accumulator (its sample count grows)
+        bool one_mesh = false;       // the scene has one mesh (plan-and-compact kernels run)
         KernelTimes times;
         std::chrono::steady_clock::time_point t0;
         virtual ~PassJob() = default;
@@ -1403,6 +1404,7 @@ std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, cons
         job->t0 = std::chrono::steady_clock::now();
         job->s = s;
         job->counts_samples = !target.moments && !target.list;
+        job->one_mesh = s->meshes.size() == 1;
         if (o.samples_per_pixel < 1)
         {
                 fail(NT_EINVAL, "Stratified jittered sample count is not a positive integer");
@@ -1505,6 +1507,7 @@ void finish_pass(PassJob& job, const nt_render_opts& o, nt_stats* st, bool copy_
                 st->extend_ms = times.extend_ms;
                 st->shade_ms = times.shade_ms;
                 st->shadow_ms = times.shadow_ms;
+                st->plan_ms = times.plan_ms;
                 st->launches = times.launches;
                 st->extend_launches = times.extend_launches;
                 st->shadow_launches = times.shadow_launches;
@@ -2551,7 +2554,8 @@ int nt_render_batch(nt_scene* const* scenes, int count, const nt_render_opts* op
                         {
                                 all &= scenes[i]->host_counters[C_DONE] != 0;
                                 err |= scenes[i]->host_counters[C_ERROR] != 0;
-                                jobs[i]->times.launches += (long long)per * Wavefront<3>::iteration_launches(jobs[i]->smooth);
+                                jobs[i]->times.launches +=
+                                        (long long)per * Wavefront<3>::iteration_launches(jobs[i]->smooth, jobs[i]->one_mesh);
                                 jobs[i]->times.extend_launches += per;
                                 jobs[i]->times.shadow_launches += per;
                         }

@@ -37,7 +37,7 @@ EXPORTED_SYMBOLS = (
     "nt_scene_object_count", "nt_accum_read_srgb_slice", "nt_convex_hull", "nt_hull_facet_count", "nt_hull_facets",
     "nt_hull_destroy", "nt_scene_clear_lights", "nt_render_batch",
     "nt_autotune", "nt_scene_set_object_surface", "nt_render_aux",
-    "nt_render_moments", "nt_render_noalloc", "nt_render_pixels",
+    "nt_render_moments", "nt_render_noalloc", "nt_render_pixels", "nt_probe_peaks",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
     "nt_denoiser_set_params", "nt_denoiser_set_input", "nt_denoiser_apply", "nt_denoiser_gradient",
     "nt_denoiser_train_step", "nt_tc_gemm_bf16", "nt_tc_gemm_wait_selftest",
@@ -75,10 +75,22 @@ class Stats(ctypes.Structure):
                 ("extend_launches", ctypes.c_int64), ("shadow_launches", ctypes.c_int64),
                 ("shadow_facet_tests", ctypes.c_int64), ("shadow_box_steps", ctypes.c_int64),
                 ("shadow_retests", ctypes.c_int64), ("shadow_descent_levels", ctypes.c_int64),
-                ("iterations", ctypes.c_int64)]
+                ("iterations", ctypes.c_int64), ("plan_ms", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class Peaks(ctypes.Structure):
+    _fields_ = [("l2_read_gbs", ctypes.c_double), ("fp32_fma_tflops", ctypes.c_double), ("l2_ms", ctypes.c_double),
+                ("fma_ms", ctypes.c_double)]
+
+
+def probe_peaks() -> dict:
+    """L2 read bandwidth (GB/s) and FP32 FMA rate (TFLOP/s) of the current GPU (nt_probe_peaks)."""
+    p = Peaks()
+    _check(library().nt_probe_peaks(ctypes.byref(p)))
+    return {name: getattr(p, name) for name, _ in Peaks._fields_}
 
 
 class MeshInfo(ctypes.Structure):
@@ -155,6 +167,7 @@ def library() -> ctypes.CDLL:
         "nt_render_aux": ([vp, vp, vp, vp], ctypes.c_int),
         "nt_render_moments": ([vp, ctypes.POINTER(RenderOpts), i64, vp, vp, ctypes.POINTER(Stats)], ctypes.c_int),
         "nt_render_pixels": ([vp, ctypes.POINTER(RenderOpts), vp, i64, vp, ctypes.POINTER(Stats)], ctypes.c_int),
+        "nt_probe_peaks": ([ctypes.POINTER(Peaks)], ctypes.c_int),
     }
     for name, (args, res) in sig.items():
         fn = getattr(lib, name)

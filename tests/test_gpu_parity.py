@@ -113,14 +113,17 @@ def test_closest_hit_bit_exact_against_oracle_fresh_rays(require_gpu, port, n, p
     pf, pt, _ = port.trace(port.mesh(n, verts, facets, dbl=True), org, dirs)
     assert st["error_bits"] == 0
     bad = np.nonzero(facet != pf)[0]
-    assert len(bad) <= 1e-4 * len(org)
+    # no allowance: every difference must be shown by exact arithmetic to be the oracle's mistake
     for i in bad:
-        assert facet[i] >= 0
-        t_gpu = _exact_hit(verts, facets[facet[i]], org[i], dirs[i])
-        assert t_gpu is not None, i
-        if pf[i] >= 0:
-            t_oracle = _exact_hit(verts, facets[pf[i]], org[i], dirs[i])
-            assert t_oracle is None or t_gpu < t_oracle, i
+        if facet[i] >= 0:
+            t_gpu = _exact_hit(verts, facets[facet[i]], org[i], dirs[i])
+            assert t_gpu is not None, i
+            if pf[i] >= 0:
+                t_oracle = _exact_hit(verts, facets[pf[i]], org[i], dirs[i])
+                assert t_oracle is None or t_gpu < t_oracle, i
+        else:
+            assert _exact_hit(verts, facets[pf[i]], org[i], dirs[i]) is None, i
+    print(f"n={n}: {len(org)} fresh rays, {len(bad)} differences from the FP64 oracle, each explained exactly")
     same = (facet == pf) & (facet >= 0)
     assert np.allclose(t[same], pt[same], rtol=2e-6, atol=0)
 
