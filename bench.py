@@ -245,7 +245,8 @@ def measure_plain(scene, spec: dict, args, steps: int, rank: int, world: int, lo
         return distributed.sample_offset(rank, k, spp_eff, world)
 
     ropts = dict(max_depth=depth, seed=spec["seed"], pool_paths=tuned["pool_paths"],
-                 graph_iterations=tuned["graph_iterations"], walk_chunk=tuned["walk_chunk"])
+                 graph_iterations=tuned["graph_iterations"], walk_chunk=tuned["walk_chunk"],
+                 walk_small_leaf=tuned["walk_small_leaf"])
 
     # warm-up (the last one is also the per-kernel timing pass: device events around every launch)
     for _ in range(args.warmup - 1):
@@ -481,7 +482,8 @@ def main() -> None:
         "config": config_block(spec, args),
         "mesh": mesh_block(spec, "exact (nt_convex_hull)"),
         "tuning": {"pool_paths": tuned["pool_paths"], "graph_iterations": tuned["graph_iterations"],
-                   "walk_chunk": tuned["walk_chunk"], "tuned_by": "nt_autotune"},
+                   "walk_chunk": tuned["walk_chunk"], "walk_small_leaf": tuned["walk_small_leaf"],
+                   "tuned_by": "nt_autotune"},
         "e2e": m["e2e"],
         "gpu_launches": m["launches"],
         "roofline": roofline(n, timed, args.config, tuned["pool_paths"], probes),
@@ -517,7 +519,8 @@ def main() -> None:
                         "mesh": mesh_block(sp, "exact (nt_convex_hull)"),
                         "tuning": {"pool_paths": mm["tuned"]["pool_paths"],
                                    "graph_iterations": mm["tuned"]["graph_iterations"],
-                                   "walk_chunk": mm["tuned"]["walk_chunk"]},
+                                   "walk_chunk": mm["tuned"]["walk_chunk"],
+                                   "walk_small_leaf": mm["tuned"]["walk_small_leaf"]},
                         "roofline": roofline(sp["n"], mm["timed"], c, mm["tuned"]["pool_paths"], probes),
                         "kernels_ms_per_frame": {kk: mm["timed"][kk + "_ms"] for kk in ("raygen", "plan", "extend",
                                                                                         "shade", "shadow")},

@@ -84,6 +84,9 @@ typedef struct nt_render_opts
                                    have their records staged in shared memory at once (cp.async); 0: the
                                    default (1).  A tuning choice only: every variant makes the same
                                    decisions.  nt_autotune picks it. */
+        int walk_small_leaf;    /* tree-walk kernels: a warp whose lanes' leaves hold at most this many facets each
+                                   tests them lane by lane instead of pooling them across the warp; 0: the default
+                                   (2); -1: always pooled.  A tuning choice only.  nt_autotune picks it. */
 } nt_render_opts;
 
 typedef struct nt_stats
@@ -259,9 +262,10 @@ int nt_accum_clear(nt_scene* scene);
 int nt_render_batch(nt_scene* const* scenes, int count, const nt_render_opts* opts, nt_stats* stats);
 
 /* Times probe passes of `base` (its samples per pixel) over candidate path-pool sizes and iterations
- * per graph launch, then over the walk kernels' variants (walk_chunk 1, 32, 64, 128) at the best
- * of those, and returns the fastest in *tuned (a copy of base with pool_paths, graph_iterations and
- * walk_chunk set) and its pass time in *best_ms (may be NULL).  The probe passes go to the scene's
+ * per graph launch, then over the walk kernels' variants (walk_chunk 1, 32, 64, 128) and small-leaf
+ * thresholds (walk_small_leaf -1, 1, 2, 4) at the best of those, and returns the fastest in *tuned (a
+ * copy of base with pool_paths, graph_iterations, walk_chunk and walk_small_leaf set) and its pass time
+ * in *best_ms (may be NULL).  The probe passes go to the scene's
  * accumulator, which is cleared afterwards. */
 int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tuned, double* best_ms);
 

@@ -93,7 +93,8 @@ def run(count: int = 64, seed: int = 0, repeat: int = 3, cache: Path | None = No
     for sp in specs:
         t = tuned[sp["n"]]
         opts.append(dict(samples_per_pixel=sp["spp"], max_depth=5, seed=sp["seed"], pool_paths=t["pool_paths"],
-                         graph_iterations=t["graph_iterations"], walk_chunk=t["walk_chunk"]))
+                         graph_iterations=t["graph_iterations"], walk_chunk=t["walk_chunk"],
+                         walk_small_leaf=t["walk_small_leaf"]))
     paths = sum(s.pixel_count * ntrace.effective_spp(sp["n"], sp["spp"]) for s, sp in zip(built, specs))
     # warm-up, then timed passes
     ntrace.render_batch(built, opts)

@@ -1266,6 +1266,7 @@ __device__ __forceinline__ void walk_begin(Walk<N>& w, const Ray<N>& ray, float 
 // (strict < in list order, near-ties settled in FP64), so the result is the per-lane loop's.
 
 constexpr int POOL_SLOTS = 128;  // pooled tests per warp and round
+constexpr int SMALL_LEAF = 2;  // default: leaves this small are tested per lane, not pooled
 
 struct PoolSlot
 {
@@ -1331,10 +1332,18 @@ __device__ __forceinline__ void cp_async_wait_all()
 template <int N, int RR = StageFit<N>::ROUNDS>
 __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start, int cnt, const Ray<N>& ray, float ao,
                                                  long long raw, const float* raw_org, const float* raw_dir, int retest,
-                                                 float* t_best, WalkStats* ws)
+                                                 float* t_best, WalkStats* ws, int small_leaf = SMALL_LEAF)
 {
         const unsigned full = 0xffffffffu;
         const int lane = threadIdx.x & 31;
+        // small leaves (at most small_leaf facets in every lane's leaf, the common case: a walk step tests
+        // one or two facets on average) are tested by each lane on its own, in list order: the pooling's
+        // scan, owner search, shuffles and second pass would cost more than the idle lanes they save
+        if ((int)__reduce_max_sync(full, (unsigned)cnt) <= small_leaf)
+        {
+                return leaf_closest<N>(M, make_int2(start, cnt), ray, ao, Ray64Source<N>{raw_org, raw_dir, raw}, retest,
+                                       t_best, ws);
+        }
         int incl = cnt;
 #pragma unroll
         for (int d = 1; d < 32; d <<= 1)
@@ -1541,7 +1550,7 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
 template <int N, int RR = StageFit<N>::ROUNDS>
 __device__ __forceinline__ int walk_step_warp(const MeshDev<N>& M, Walk<N>& w, bool active, int retest,
                                               const float* raw_org, const float* raw_dir, float* t_out, int* facet_out,
-                                              WalkStats* ws)
+                                              WalkStats* ws, int small_leaf = SMALL_LEAF)
 {
         int status = W_MISS;
         bool leaf = false;
@@ -1577,7 +1586,8 @@ __device__ __forceinline__ int walk_step_warp(const MeshDev<N>& M, Walk<N>& w, b
         }
         const int cnt = (leaf && nd.y > 0) ? nd.y : 0;
         float t = FLT_MAX;
-        const int f = leaf_closest_warp<N, RR>(M, nd.x, cnt, w.ray, w.ao, w.raw, raw_org, raw_dir, retest, &t, ws);
+        const int f = leaf_closest_warp<N, RR>(M, nd.x, cnt, w.ray, w.ao, w.raw, raw_org, raw_dir, retest, &t, ws,
+                                                small_leaf);
         if (status != W_RUNNING)
         {
                 return status;

@@ -142,6 +142,8 @@ struct DevScene
         int retest;          // 1: FP64 re-test of uncertain facet tests
         int walk_rounds;     // walk kernels: rounds of 32 pooled facet tests staged per warp chunk (1, 2
                              // or 4; 0: the default for N); host-side choice of the kernel variant
+        int walk_small;      // walk kernels: leaves of at most this many facets (in every lane of a warp)
+                             // are tested per lane instead of pooled across the warp
 };
 
 // Render-pass constants.

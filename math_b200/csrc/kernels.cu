@@ -894,7 +894,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                 {
                         float t = 0;
                         int f = -1;
-                        int status = walk_step_warp<N, R>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
+                        int status = walk_step_warp<N, R>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws, S.walk_small);
                         if (i >= 0 && status != W_RUNNING)
                         {
                                 float tt;
@@ -1001,7 +1001,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                 {
                         float t = 0;
                         int f = -1;
-                        int status = walk_step_warp<N, R>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws);
+                        int status = walk_step_warp<N, R>(M, w, i >= 0, S.retest, nullptr, nullptr, &t, &f, &ws, S.walk_small);
                         if (i >= 0 && status != W_RUNNING)
                         {
                                 if (!(status == W_HIT && t < dist))

@@ -1377,6 +1377,16 @@ int walk_rounds(const nt_render_opts& o)
         return o.walk_chunk == 1 ? -1 : o.walk_chunk / 32;
 }
 
+// The walk kernels' small-leaf threshold (nt_render_opts.walk_small_leaf; 0: the default).
+int walk_small(const nt_render_opts& o)
+{
+        if (o.walk_small_leaf < -1 || o.walk_small_leaf > 64)
+        {
+                fail(NT_EINVAL, "walk_small_leaf must be -1..64");
+        }
+        return o.walk_small_leaf == 0 ? 2 : (o.walk_small_leaf < 0 ? 0 : o.walk_small_leaf);
+}
+
 // Where a pass's radiance goes when it is not the scene's per-pixel accumulator.
 struct PassTarget
 {
@@ -1424,6 +1434,7 @@ std::unique_ptr<PassJob> prepare_pass(nt_scene* s, const nt_render_opts& o, cons
         S.max_depth = o.max_depth;
         S.retest = o.retest;
         S.walk_rounds = walk_rounds(o);
+        S.walk_small = walk_small(o);
         const bool smooth = smooth_shading(s, o);
         S.smooth_normal = smooth ? 1 : 0;
         const long long npix = s->pixel_count();
@@ -1597,6 +1608,7 @@ void render_noalloc(nt_scene* s, const nt_render_opts& o, double* d_accum, long 
         S.retest = o.retest;
         S.smooth_normal = smooth ? 1 : 0;
         S.walk_rounds = walk_rounds(o);
+        S.walk_small = walk_small(o);
         unsigned long long* counters = static_cast<unsigned long long*>(scratch);
         Wavefront<N> W;
         W.carve(static_cast<char*>(scratch) + head, Q, lights, smooth);
@@ -2617,12 +2629,15 @@ int nt_autotune(nt_scene* scene, const nt_render_opts* base, nt_render_opts* tun
                                 }
                         }
                 }
-                // then the walk kernels' staging chunk at the best pool and iterations
+                // then the walk kernels' variant and small-leaf threshold at the best pool and iterations
                 const nt_render_opts at = best;
-                for (int chunk : {1, 32, 64, 128})
+                for (int v = 0; v < 7; ++v)
                 {
                         nt_render_opts o = at;
-                        o.walk_chunk = chunk;
+                        static const int chunks[7] = {1, 32, 64, 128, 1, 1, 1};
+                        static const int smalls[7] = {2, 2, 2, 2, -1, 1, 4};
+                        o.walk_chunk = chunks[v];
+                        o.walk_small_leaf = smalls[v];
                         o.timing = 0;
                         o.stop = nullptr;
                         for (int rep = 0; rep < 2; ++rep)

@@ -63,7 +63,7 @@ class RenderOpts(ctypes.Structure):
     _fields_ = [("samples_per_pixel", ctypes.c_int), ("max_depth", ctypes.c_int), ("seed", ctypes.c_uint64),
                 ("retest", ctypes.c_int), ("smooth_normal", ctypes.c_int), ("pool_paths", ctypes.c_int64),
                 ("timing", ctypes.c_int), ("stop", ctypes.c_void_p), ("graph_iterations", ctypes.c_int),
-                ("sample_offset", ctypes.c_int64), ("walk_chunk", ctypes.c_int)]
+                ("sample_offset", ctypes.c_int64), ("walk_chunk", ctypes.c_int), ("walk_small_leaf", ctypes.c_int)]
 
 
 class Stats(ctypes.Structure):
@@ -225,10 +225,11 @@ def cosine_sphere_coefficient(n: int) -> float:
 
 def render_opts(samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                 smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False,
-                graph_iterations: int = 0, sample_offset: int = 0, walk_chunk: int = 0) -> RenderOpts:
+                graph_iterations: int = 0, sample_offset: int = 0, walk_chunk: int = 0,
+                walk_small_leaf: int = 0) -> RenderOpts:
     return RenderOpts(int(samples_per_pixel), int(max_depth), int(seed) & (2 ** 64 - 1), int(bool(retest)),
                       int(bool(smooth_normal)), int(pool_paths), int(bool(timing)), None, int(graph_iterations),
-                      int(sample_offset), int(walk_chunk))
+                      int(sample_offset), int(walk_chunk), int(walk_small_leaf))
 
 
 def render_batch(scenes: list, opts: list[dict]) -> list[dict]:
@@ -368,11 +369,12 @@ class Scene:
 
     def render(self, samples_per_pixel: int, max_depth: int = 100, seed: int = 0, retest: bool = True,
                smooth_normal: bool = False, pool_paths: int = 0, timing: bool = False, stop=None,
-               graph_iterations: int = 0, sample_offset: int = 0, walk_chunk: int = 0) -> dict:
+               graph_iterations: int = 0, sample_offset: int = 0, walk_chunk: int = 0,
+               walk_small_leaf: int = 0) -> dict:
         """One pass added to the accumulator (nt_render); sample_offset > 0 starts it at that sample
         index, 0 continues after the accumulated samples."""
         o = render_opts(samples_per_pixel, max_depth, seed, retest, smooth_normal, pool_paths, timing,
-                        graph_iterations, sample_offset, walk_chunk)
+                        graph_iterations, sample_offset, walk_chunk, walk_small_leaf)
         if stop is not None:
             o.stop = ctypes.cast(stop, ctypes.c_void_p)
         st = Stats()
@@ -407,7 +409,7 @@ class Scene:
         ms = ctypes.c_double()
         _check(self._lib.nt_autotune(self._h, ctypes.byref(base), ctypes.byref(out), ctypes.byref(ms)))
         return {"pool_paths": int(out.pool_paths), "graph_iterations": int(out.graph_iterations),
-                "walk_chunk": int(out.walk_chunk)}, float(ms.value)
+                "walk_chunk": int(out.walk_chunk), "walk_small_leaf": int(out.walk_small_leaf)}, float(ms.value)
 
     def clear(self) -> None:
         _check(self._lib.nt_accum_clear(self._h))

@@ -43,13 +43,14 @@ def test_graph_and_direct_iterations_trace_the_same_paths(require_gpu):
 @pytest.mark.parametrize("name", ["n3_small", "n4_small", "n5_small", "n6_small"])
 def test_walk_chunks_trace_the_same_paths(require_gpu, name):
     """The walk kernels' variant (records read directly, or staged in chunks of 32, 64 or 128 pooled
-    facet tests per warp) is a tuning choice only: every variant makes the same decisions (same work
+    facet tests per warp) and small-leaf threshold (leaves tested lane by lane below it, pooled across
+    the warp above it) are tuning choices only: every combination makes the same decisions (same work
     counters, same image)."""
     spec, s = _scene(name)
     ref = None
-    for chunk in (1, 32, 64, 128):
+    for chunk, small in ((1, 2), (32, 2), (64, 2), (128, 2), (1, -1), (1, 4), (32, 8)):
         s.clear()
-        st = s.render(spec["spp"], max_depth=spec["max_depth"], seed=6, walk_chunk=chunk)
+        st = s.render(spec["spp"], max_depth=spec["max_depth"], seed=6, walk_chunk=chunk, walk_small_leaf=small)
         img, _ = s.image()
         assert st["error_bits"] == 0
         if ref is None:
@@ -57,8 +58,8 @@ def test_walk_chunks_trace_the_same_paths(require_gpu, name):
             continue
         for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests", "shadow_facet_tests",
                   "shadow_box_steps"):
-            assert st[k] == ref[0][k], (chunk, k)
-        assert rrmse(img, ref[1]) < 1e-12, chunk
+            assert st[k] == ref[0][k], (chunk, small, k)
+        assert rrmse(img, ref[1]) < 1e-12, (chunk, small)
 
 
 def test_walk_chunk_is_validated(require_gpu):
