@@ -318,38 +318,12 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_extend(__grid_consta
         flush_stats<false>(counters, ws, rays, 0);
 }
 
-// Adds a path's radiance to its pixel.  Consecutive paths of a queue are mostly samples of the same
-// pixel, so the lanes that reach this call together first combine their contributions per pixel (the
-// lowest lane of each group of equal pixels sums its group's values, in lane order, over shuffles) and
-// one lane per pixel issues the three FP64 atomics: atomics on one address from many lanes would be
-// serialised at the L2.
 __device__ __forceinline__ void accumulate(double* accum, uint32_t pixel, float r, float g, float b)
 {
-        const unsigned mask = __activemask();
-        const unsigned peers = __match_any_sync(mask, pixel);
-        const int lane = threadIdx.x & 31;
-        const int leader = __ffs(peers) - 1;
-        double sr = r, sg = g, sb = b;
-        if (peers != (1u << lane))
-        {
-                for (unsigned m = peers & (peers - 1); m; m &= m - 1)
-                {
-                        const int src = __ffs(m) - 1;
-                        const float vr = __shfl_sync(peers, r, src);
-                        const float vg = __shfl_sync(peers, g, src);
-                        const float vb = __shfl_sync(peers, b, src);
-                        sr += vr;
-                        sg += vg;
-                        sb += vb;
-                }
-        }
-        if (lane == leader)
-        {
-                double* p = accum + (size_t)pixel * 3;
-                atomicAdd(p + 0, sr);
-                atomicAdd(p + 1, sg);
-                atomicAdd(p + 2, sb);
-        }
+        double* p = accum + (size_t)pixel * 3;
+        atomicAdd(p + 0, (double)r);
+        atomicAdd(p + 1, (double)g);
+        atomicAdd(p + 2, (double)b);
 }
 
 // shading: trace_path / direct_diffuse_lighting / diffuse_lighting (painter.cpp:197-397).  A miss
