@@ -16,6 +16,7 @@ from __future__ import annotations
 import argparse
 import json
 import math
+import os
 import sys
 import time
 from pathlib import Path
@@ -52,7 +53,7 @@ def make_workload(count: int, seed: int, cache: Path | None = None, max_points: 
     """`count` seeded scenes: n uniform in {3, 4, 5, 6}, point counts log-uniform in POINT_RANGE[n] (capped
     at max_points), screens log-uniform in SCREEN_RANGE[n], 1 to 16 samples per pixel."""
     rng = np.random.default_rng(seed)
-    specs = []
+    plans = []
     for i in range(count):
         n = int(rng.integers(3, 7))
         plo, phi = POINT_RANGE[n]
@@ -62,7 +63,17 @@ def make_workload(count: int, seed: int, cache: Path | None = None, max_points: 
         lo, hi = SCREEN_RANGE[n]
         screen = int(round(math.exp(rng.uniform(math.log(lo), math.log(hi)))))
         spp = int(rng.integers(1, 17))
-        v, f = scene_mesh(n, points, seed * 1000 + i, cache)
+        plans.append((n, points, screen, spp, i))
+    # the hulls on host threads (the library's hull call releases the interpreter lock), largest first
+    from concurrent.futures import ThreadPoolExecutor
+
+    order = sorted(range(count), key=lambda k: -plans[k][1] * 2 ** plans[k][0])
+    with ThreadPoolExecutor(max_workers=max(1, min(16, os.cpu_count() or 1))) as ex:
+        meshes = dict(zip(order, ex.map(lambda k: scene_mesh(plans[k][0], plans[k][1], seed * 1000 + plans[k][4], cache),
+                                        order)))
+    specs = []
+    for k, (n, points, screen, spp, i) in enumerate(plans):
+        v, f = meshes[k]
         spec = scenes.make_spec(n, v, f, screen=screen, spp=spp, max_depth=5, seed=i)
         spec["points"] = points
         specs.append(spec)
