@@ -297,6 +297,10 @@ def measure_plain(scene, spec: dict, args, steps: int, rank: int, world: int, lo
         # read back; wall clock around the calls, the first step's copy included
         scene.clear()
         host_img = torch.empty((scene.pixel_count, 3), dtype=torch.float32, pin_memory=True).numpy()
+        # one untimed round of the upload path first: its first call creates the copy stream and
+        # allocates the device staging buffers (set-up, not per-frame work)
+        scene.upload_begin()
+        scene.upload_commit()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         e2e_paths = 0
