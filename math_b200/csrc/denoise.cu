@@ -55,6 +55,12 @@ __device__ __forceinline__ uint32_t smem_u32(const void* p)
         return (uint32_t)__cvta_generic_to_shared(p);
 }
 
+// one 16-byte global -> shared copy that does not pass through registers (cp.async, L2 only)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem)
+{
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_u32(smem)), "l"(gmem) : "memory");
+}
+
 // byte offset of element (r, k) of a GK-wide K-major tile: core matrices of 8 rows x 16 bytes, the
 // K direction first (leading byte offset 128), then the next 8 rows (stride byte offset GK / 8 x 128)
 __device__ __forceinline__ uint32_t tile_off(int r, int k)
@@ -180,18 +186,22 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
         {
                 if constexpr (LA::VEC8)
                 {
-                        // 16-byte chunks, eight consecutive rows fastest: a quarter warp's stores fill
-                        // one 128-byte block of core-matrix rows (no bank conflicts)
+                        // 16-byte chunks copied global -> shared with cp.async (every chunk of the tile in
+                        // flight at once; a chunk of eight K lies whole in a core-matrix row), eight
+                        // consecutive rows fastest: a quarter warp fills one 128-byte block of
+                        // core-matrix rows (no bank conflicts); chunks outside the matrix are zeroed
                         for (int idx = tid; idx < GM * (GK / 8); idx += GTHREADS)
                         {
                                 const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
                                 const int k8 = ((idx >> 3) % (GK / 8)) * 8;
-                                uint4 v = make_uint4(0u, 0u, 0u, 0u);
                                 if (m0 + r < M && kc + k8 < ke)
                                 {
-                                        v = la.load8(m0 + r, kc + k8);
+                                        cp_async16(sA + tile_off(r, k8), la.addr8(m0 + r, kc + k8));
                                 }
-                                *reinterpret_cast<uint4*>(sA + tile_off(r, k8)) = v;
+                                else
+                                {
+                                        *reinterpret_cast<uint4*>(sA + tile_off(r, k8)) = make_uint4(0u, 0u, 0u, 0u);
+                                }
                         }
                 }
                 else if (LA::ROW_FAST)
@@ -218,13 +228,20 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
                         {
                                 const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
                                 const int k8 = ((idx >> 3) % (GK / 8)) * 8;
-                                uint4 v = make_uint4(0u, 0u, 0u, 0u);
                                 if (kc + k8 < ke)
                                 {
-                                        v = lb.load8(r, kc + k8);
+                                        cp_async16(sB + tile_off(r, k8), lb.addr8(r, kc + k8));
                                 }
-                                *reinterpret_cast<uint4*>(sB + tile_off(r, k8)) = v;
+                                else
+                                {
+                                        *reinterpret_cast<uint4*>(sB + tile_off(r, k8)) = make_uint4(0u, 0u, 0u, 0u);
+                                }
                         }
+                }
+                if constexpr (LA::VEC8 || LB::VEC8)
+                {
+                        asm volatile("cp.async.commit_group;" ::: "memory");
+                        asm volatile("cp.async.wait_group 0;" ::: "memory");
                 }
                 else if (LB::ROW_FAST)
                 {
@@ -324,6 +341,10 @@ struct LoadRows
         __device__ __forceinline__ uint4 load8(int r, int k) const
         {
                 return __ldg(reinterpret_cast<const uint4*>(p + (size_t)r * ld + k));
+        }
+        __device__ __forceinline__ const void* addr8(int r, int k) const
+        {
+                return p + (size_t)r * ld + k;
         }
         bool vec8_ok() const
         {
