@@ -77,6 +77,13 @@ int nt_denoiser_train_step(nt_denoiser* d, const float* d_target, float lr, doub
  * N <= 256.  stream: a cudaStream_t or NULL (the default stream). */
 int nt_tc_gemm_bf16(const uint16_t* d_a, const uint16_t* d_b, float* d_c, int m, int n, int k, void* stream);
 
+/* The same GEMM in the form of the network's weight gradients: C[M x N] = At^T Bt with At (K x M) and
+ * Bt (K x N) row-major BF16, i.e. both operands transposed (read MN-major), the K range split over CTAs
+ * of k_per_cta each (0: one CTA per row block) whose partial sums are added into C with FP32 atomics
+ * (C is zeroed first).  M a multiple of 8; N a multiple of 16, at most 256. */
+int nt_tc_gemm_bf16_t(const uint16_t* d_at, const uint16_t* d_bt, float* d_c, int m, int n, int k, int k_per_cta,
+                      void* stream);
+
 /* Failure-detection self-test of the GEMM kernel: one small launch with its tensor-core instructions
  * withheld, so that the kernel's bounded wait for their completion (20 ms here, about a second in
  * ordinary launches) runs out; the kernel then gives its tensor memory back, raises its error flag and

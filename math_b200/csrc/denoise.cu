@@ -1,14 +1,14 @@
 // Learned kernel-predicting denoiser (include/ntrace_denoise.h) on the sm_100a tensor cores.
 //
-// The network's matrix products run in one GEMM kernel built on tcgen05: operand tiles are staged
-// by the CTA's threads into shared memory in the canonical K-major layout without swizzle (8 x 16-byte
-// core matrices), one elected thread issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in
-// tensor memory) and commits to an mbarrier, and the epilogue reads the accumulator back with
-// tcgen05.ld and applies a fused bias / ReLU / mask / store or atomic reduction.  Operand loaders
-// gather from any layout (row-major, transposed, or the feature stencil computed on the fly), so the
-// forward pass, the backward data products and the weight gradients (a reduction over pixels, split
-// across CTAs) all use the same kernel.  The rest (features, softmax filters, loss, bias sums, Adam)
-// are plain CUDA-core kernels.
+// The network's matrix products run in one GEMM kernel built on tcgen05: operand tiles are copied
+// global -> shared with cp.async in 16-byte chunks, into the canonical layouts without swizzle (8 x
+// 16-byte core matrices), K-major for row-major operands and MN-major for transposed ones, two stages
+// deep; one elected thread issues tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in tensor
+// memory) and commits to the stage's mbarrier, and the epilogue reads the accumulator back with
+// tcgen05.ld and applies a fused bias / ReLU / mask / store or atomic reduction.  The forward pass,
+// the backward data products and the weight gradients (a reduction over pixels, split across CTAs)
+// all use the same kernel.  The rest (features, softmax filters, loss, bias sums, Adam) are plain
+// CUDA-core kernels.
 #include "ntrace.h"
 #include "ntrace_denoise.h"
 
@@ -139,25 +139,85 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v)
         }
 }
 
+// byte offset of element (r, k) of a GK-wide MN-major tile: core matrices of 8 k x 16 bytes (eight
+// consecutive rows), k fastest (leading byte offset 128 between groups of eight k), then the next
+// eight rows (stride byte offset GK x 16)
+__device__ __forceinline__ uint32_t tile_off_mn(int r, int k)
+{
+        return (uint32_t)((r >> 3) * (GK * 16) + k * 16 + (r & 7) * 2);
+}
+
+// Copies the GK-wide slice [kc, kc + GK) of rows [r0, r0 + rows) of an operand into a shared-memory
+// tile with cp.async, one 16-byte chunk per copy (every chunk of the tile in flight at once); chunks
+// outside the operand (row >= rmax or k >= ke) are zeroed.
+//  * K-major operands (L::MN_MAJOR false): a chunk is eight consecutive k of one row, and eight
+//    consecutive rows go fastest, so that a quarter warp fills one 128-byte block of core-matrix rows
+//    (no bank conflicts).
+//  * MN-major operands (the transpose of a row-major matrix): a chunk is eight consecutive rows at one
+//    k; two threads take sixteen rows (one 32-byte sector), and consecutive pairs consecutive k, so
+//    that a warp's 32 chunks spread over all 32 banks.
+template <class L>
+__device__ __forceinline__ void fill_tile(const L& ld, unsigned char* s, int rows, int r0, int rmax, int kc, int ke)
+{
+        if constexpr (!L::MN_MAJOR)
+        {
+                for (int idx = threadIdx.x; idx < rows * (GK / 8); idx += GTHREADS)
+                {
+                        const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
+                        const int k8 = ((idx >> 3) % (GK / 8)) * 8;
+                        unsigned char* dst = s + tile_off(r, k8);
+                        if (r0 + r < rmax && kc + k8 < ke)
+                        {
+                                cp_async16(dst, ld.addr8(r0 + r, kc + k8));
+                        }
+                        else
+                        {
+                                *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
+                        }
+                }
+        }
+        else
+        {
+                for (int idx = threadIdx.x; idx < (rows / 8) * GK; idx += GTHREADS)
+                {
+                        const int k = (idx >> 1) % GK;
+                        const int r = ((idx >> 1) / GK) * 16 + (idx & 1) * 8;
+                        unsigned char* dst = s + tile_off_mn(r, k);
+                        if (r0 + r < rmax && kc + k < ke)
+                        {
+                                cp_async16(dst, ld.addr8(r0 + r, kc + k));
+                        }
+                        else
+                        {
+                                *reinterpret_cast<uint4*>(dst) = make_uint4(0u, 0u, 0u, 0u);
+                        }
+                }
+        }
+}
+
 // C[M x N] = sum_k A(m, k) B(n, k) over k in this CTA's K range [blockIdx.y * k_per_cta, ...).
-// LA / LB: operand loaders (float operator()(row, k), ROW_FAST: consecutive threads take consecutive
-// rows rather than consecutive k); EPI: epilogue (row, first column, 16 values).  N: multiple of 16,
-// at most 256; ncols: tensor-memory columns (power of two >= max(32, N)).
+// LA / LB: operand loaders (LoadRows: K-major, LoadCols: MN-major); EPI: epilogue (row, first column,
+// 16 values).  N: multiple of 16, at most 256; ncols: tensor-memory columns (power of two >= max(32, N)).
+//
+// Two shared-memory stages: while the tensor core multiplies chunk i out of one stage, the threads
+// copy chunk i + 1 into the other, once the MMAs of chunk i - 1 (which read it) have completed.  Each
+// stage has its own mbarrier, to which the MMA thread commits; chunk j's commit completes phase j / 2
+// of barrier j % 2.
 template <class LA, class LB, class EPI>
 __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, const EPI epi, int M, int N, int K,
                                                    int k_per_cta, uint32_t ncols, int* err, const GemmCtl ctl)
 {
         extern __shared__ __align__(1024) unsigned char g_smem[];
-        __shared__ __align__(8) unsigned long long s_bar;
+        __shared__ __align__(8) unsigned long long s_bar[2];
         __shared__ uint32_t s_tmem;
-        unsigned char* sA = g_smem;
-        unsigned char* sB = g_smem + GM * GK * 2;
         const int tid = threadIdx.x;
         const int warp = tid >> 5;
         const int lane = tid & 31;
         const int m0 = blockIdx.x * GM;
         const int kb = blockIdx.y * k_per_cta;
         const int ke = min(K, kb + k_per_cta);
+        const int stage_bytes = (GM + N) * GK * 2;  // A then B; a multiple of 2048 bytes
+        const int nk = ke > kb ? (ke - kb + GK - 1) / GK : 0;
 
         if (warp == 0)
         {
@@ -168,99 +228,32 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
         }
         if (tid == 0)
         {
-                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar)) : "memory");
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[0])) : "memory");
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_bar[1])) : "memory");
                 asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         }
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
         __syncthreads();
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t tmem = s_tmem;
-        const uint32_t idesc = umma_idesc_bf16(GM, N);
-        const uint32_t sbo = GK / 8 * 128;
+        const uint32_t idesc = umma_idesc_bf16(GM, N) | (LA::MN_MAJOR ? 1u << 15 : 0u) | (LB::MN_MAJOR ? 1u << 16 : 0u);
+        // both layouts: 128 bytes between groups of eight k, GK x 16 bytes between groups of eight rows
+        const uint32_t lbo = 128, sbo = GK * 16;
 
-        uint32_t parity = 0;
-        int stages = 0;
-        bool ok = true;
-        bool pending = false;
-        for (int kc = kb; kc < ke; kc += GK)
+        if (nk > 0)
         {
-                if constexpr (LA::VEC8)
-                {
-                        // 16-byte chunks copied global -> shared with cp.async (every chunk of the tile in
-                        // flight at once; a chunk of eight K lies whole in a core-matrix row), eight
-                        // consecutive rows fastest: a quarter warp fills one 128-byte block of
-                        // core-matrix rows (no bank conflicts); chunks outside the matrix are zeroed
-                        for (int idx = tid; idx < GM * (GK / 8); idx += GTHREADS)
-                        {
-                                const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
-                                const int k8 = ((idx >> 3) % (GK / 8)) * 8;
-                                if (m0 + r < M && kc + k8 < ke)
-                                {
-                                        cp_async16(sA + tile_off(r, k8), la.addr8(m0 + r, kc + k8));
-                                }
-                                else
-                                {
-                                        *reinterpret_cast<uint4*>(sA + tile_off(r, k8)) = make_uint4(0u, 0u, 0u, 0u);
-                                }
-                        }
-                }
-                else if (LA::ROW_FAST)
-                {
-                        for (int idx = tid; idx < GM * GK; idx += GTHREADS)
-                        {
-                                const int r = idx % GM, k = idx / GM;
-                                const float v = (m0 + r < M && kc + k < ke) ? la(m0 + r, kc + k) : 0.0f;
-                                *reinterpret_cast<__nv_bfloat16*>(sA + tile_off(r, k)) = __float2bfloat16_rn(v);
-                        }
-                }
-                else
-                {
-                        for (int idx = tid; idx < GM * GK; idx += GTHREADS)
-                        {
-                                const int r = idx / GK, k = idx % GK;
-                                const float v = (m0 + r < M && kc + k < ke) ? la(m0 + r, kc + k) : 0.0f;
-                                *reinterpret_cast<__nv_bfloat16*>(sA + tile_off(r, k)) = __float2bfloat16_rn(v);
-                        }
-                }
-                if constexpr (LB::VEC8)
-                {
-                        for (int idx = tid; idx < N * (GK / 8); idx += GTHREADS)
-                        {
-                                const int r = (idx & 7) | ((idx / (8 * (GK / 8))) << 3);
-                                const int k8 = ((idx >> 3) % (GK / 8)) * 8;
-                                if (kc + k8 < ke)
-                                {
-                                        cp_async16(sB + tile_off(r, k8), lb.addr8(r, kc + k8));
-                                }
-                                else
-                                {
-                                        *reinterpret_cast<uint4*>(sB + tile_off(r, k8)) = make_uint4(0u, 0u, 0u, 0u);
-                                }
-                        }
-                }
-                if constexpr (LA::VEC8 || LB::VEC8)
-                {
-                        asm volatile("cp.async.commit_group;" ::: "memory");
-                        asm volatile("cp.async.wait_group 0;" ::: "memory");
-                }
-                else if (LB::ROW_FAST)
-                {
-                        for (int idx = tid; idx < N * GK; idx += GTHREADS)
-                        {
-                                const int r = idx % N, k = idx / N;
-                                const float v = (kc + k < ke) ? lb(r, kc + k) : 0.0f;
-                                *reinterpret_cast<__nv_bfloat16*>(sB + tile_off(r, k)) = __float2bfloat16_rn(v);
-                        }
-                }
-                else
-                {
-                        for (int idx = tid; idx < N * GK; idx += GTHREADS)
-                        {
-                                const int r = idx / GK, k = idx % GK;
-                                const float v = (kc + k < ke) ? lb(r, kc + k) : 0.0f;
-                                *reinterpret_cast<__nv_bfloat16*>(sB + tile_off(r, k)) = __float2bfloat16_rn(v);
-                        }
-                }
+                fill_tile(la, g_smem, GM, m0, M, kb, ke);
+                fill_tile(lb, g_smem + GM * GK * 2, N, 0, N, kb, ke);
+        }
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        bool ok = true;
+        int issued = 0;  // chunks whose MMAs have been committed
+        for (int i = 0; i < nk; ++i)
+        {
+                const int b = i & 1;
+                unsigned char* sA = g_smem + b * stage_bytes;
+                unsigned char* sB = sA + GM * GK * 2;
+                asm volatile("cp.async.wait_group 0;" ::: "memory");
                 // the tensor core reads shared memory through the async proxy
                 asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
                 __syncthreads();
@@ -270,9 +263,9 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
 #pragma unroll
                         for (int s = 0; s < GK / 16; ++s)
                         {
-                                const uint64_t da = umma_desc(smem_u32(sA) + s * 256, 128, sbo);
-                                const uint64_t db = umma_desc(smem_u32(sB) + s * 256, 128, sbo);
-                                const uint32_t accumulate = (stages > 0 || s > 0) ? 1u : 0u;
+                                const uint64_t da = umma_desc(smem_u32(sA) + s * 256, lbo, sbo);
+                                const uint64_t db = umma_desc(smem_u32(sB) + s * 256, lbo, sbo);
+                                const uint32_t accumulate = (i > 0 || s > 0) ? 1u : 0u;
                                 asm volatile(
                                         "{\n\t.reg .pred p;\n\t"
                                         "setp.ne.b32 p, %4, 0;\n\t"
@@ -281,29 +274,40 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
                                         : "memory");
                         }
                         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                             smem_u32(&s_bar))
+                                             smem_u32(&s_bar[b]))
                                      : "memory");
                 }
-                pending = true;
-                // the stage is overwritten next: wait until the MMAs have read it
-                const bool done = mbar_wait(&s_bar, parity, ctl.wait_ns);
-                ok = __syncthreads_and(done) != 0;
-                if (!ok)
+                issued = i + 1;
+                if (i + 1 < nk)
                 {
-                        break;
+                        if (i >= 1)
+                        {
+                                // the other stage was read by chunk i - 1's MMAs
+                                const bool done = mbar_wait(&s_bar[b ^ 1], (uint32_t)(((i - 1) >> 1) & 1), ctl.wait_ns);
+                                ok = __syncthreads_and(done) != 0;
+                                if (!ok)
+                                {
+                                        break;
+                                }
+                        }
+                        unsigned char* nA = g_smem + (b ^ 1) * stage_bytes;
+                        const int kn = kb + (i + 1) * GK;
+                        fill_tile(la, nA, GM, m0, M, kn, ke);
+                        fill_tile(lb, nA + GM * GK * 2, N, 0, N, kn, ke);
+                        asm volatile("cp.async.commit_group;" ::: "memory");
                 }
-                pending = false;
-                parity ^= 1u;
-                ++stages;
         }
-        if (!ok && pending)
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        if (issued > 0)
         {
-                // a commit that did not arrive in time: wait once more (bounded) before the
-                // accumulator's columns are given back
-                mbar_wait(&s_bar, parity, ctl.wait_ns);
+                // the last chunk's MMAs (and with them every earlier one) before the accumulator is read
+                // or its columns are given back; after a wait that ran out, once more (bounded)
+                const int j = issued - 1;
+                const bool done = mbar_wait(&s_bar[j & 1], (uint32_t)((j >> 1) & 1), ctl.wait_ns);
+                ok = (__syncthreads_and(done) != 0) && ok;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (ok && stages > 0)
+        if (ok && issued > 0)
         {
                 const int row = m0 + warp * 32 + lane;
                 for (int c = 0; c < N; c += 16)
@@ -331,36 +335,37 @@ __global__ void __launch_bounds__(GTHREADS) k_gemm(const LA la, const LB lb, con
 
 // ---- operand loaders ----
 
-// A(r, k) = p[r * ld + k], BF16; VEC8: eight consecutive k (k a multiple of 8) as one 16-byte load,
-// which needs p 16-byte aligned and ld a multiple of 8
+// A(r, k) = p[r * ld + k], BF16, K-major: eight consecutive k (k a multiple of 8) are one 16-byte
+// chunk, which needs p 16-byte aligned and ld a multiple of 8
 struct LoadRows
 {
-        static constexpr bool VEC8 = true;
+        static constexpr bool MN_MAJOR = false;
         const __nv_bfloat16* p;
         int ld;
-        __device__ __forceinline__ uint4 load8(int r, int k) const
-        {
-                return __ldg(reinterpret_cast<const uint4*>(p + (size_t)r * ld + k));
-        }
         __device__ __forceinline__ const void* addr8(int r, int k) const
         {
                 return p + (size_t)r * ld + k;
         }
-        bool vec8_ok() const
+        bool chunks_ok() const
         {
                 return ((uintptr_t)p & 15u) == 0 && ld % 8 == 0;
         }
 };
 
-struct LoadCols  // A(r, k) = p[k * ld + r], BF16 (the transpose of a row-major matrix)
+// A(r, k) = p[k * ld + r], BF16 (the transpose of a row-major matrix), MN-major: eight consecutive
+// rows (r a multiple of 8) are one 16-byte chunk, which needs p 16-byte aligned and ld a multiple of 8
+struct LoadCols
 {
-        static constexpr bool ROW_FAST = true;
-        static constexpr bool VEC8 = false;
+        static constexpr bool MN_MAJOR = true;
         const __nv_bfloat16* p;
         int ld;
-        __device__ __forceinline__ float operator()(int r, int k) const
+        __device__ __forceinline__ const void* addr8(int r, int k) const
         {
-                return __bfloat162float(p[(size_t)k * ld + r]);
+                return p + (size_t)k * ld + r;
+        }
+        bool chunks_ok() const
+        {
+                return ((uintptr_t)p & 15u) == 0 && ld % 8 == 0;
         }
 };
 
@@ -560,26 +565,18 @@ cudaError_t gemm(const LA& la, const LB& lb, const EPI& epi, int M, int N, int K
         {
                 return cudaErrorInvalidValue;
         }
-        // 16-byte operand chunks lie wholly inside or outside a CTA's K range when K is a multiple of 8
-        if constexpr (LA::VEC8)
+        // 16-byte operand chunks: a K-major chunk lies wholly inside or outside a CTA's K range when K
+        // is a multiple of 8, an MN-major one inside or outside the rows when M (N) is
+        if (!la.chunks_ok() || !lb.chunks_ok() || (!LA::MN_MAJOR && K % 8 != 0) || (!LB::MN_MAJOR && K % 8 != 0) ||
+            (LA::MN_MAJOR && M % 8 != 0))
         {
-                if (!la.vec8_ok() || K % 8 != 0)
-                {
-                        return cudaErrorInvalidValue;
-                }
-        }
-        if constexpr (LB::VEC8)
-        {
-                if (!lb.vec8_ok() || K % 8 != 0)
-                {
-                        return cudaErrorInvalidValue;
-                }
+                return cudaErrorInvalidValue;
         }
         const uint32_t ncols = tmem_cols(N);
         // at most 512 / ncols CTAs share an SM's tensor memory: ask for enough shared memory that no
         // more are resident (an allocation then never waits)
         const int per_sm = 512 / (int)ncols;
-        const size_t need = (size_t)(GM + N) * GK * 2;
+        const size_t need = 2 * (size_t)(GM + N) * GK * 2;  // two stages
         const size_t smem = std::max(need, (size_t)(SM_SMEM / (per_sm + 1) + 1024));
         cudaError_t e = cudaFuncSetAttribute(k_gemm<LA, LB, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess)
@@ -1532,6 +1529,32 @@ int nt_tc_gemm_bf16(const uint16_t* d_a, const uint16_t* d_b, float* d_c, int m,
                 ck(cudaMemsetAsync(err.p, 0, sizeof(int), s), "memset");
                 ck(gemm(LoadRows{(const __nv_bfloat16*)d_a, k}, LoadRows{(const __nv_bfloat16*)d_b, k}, EpiStoreF32{d_c, n},
                         m, n, k, 0, err.as<int>(), s),
+                   "gemm");
+                int h = 0;
+                ck(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");
+                ck(cudaStreamSynchronize(s), "sync");
+                if (h)
+                {
+                        throw DError{NT_ETIMEOUT, "tensor-core GEMM: an MMA completion wait ran out"};
+                }
+        });
+}
+
+int nt_tc_gemm_bf16_t(const uint16_t* d_at, const uint16_t* d_bt, float* d_c, int m, int n, int k, int k_per_cta,
+                      void* stream)
+{
+        return guard([&]() {
+                if (!d_at || !d_bt || !d_c || m < 8 || m % 8 || n < 16 || n > 256 || n % 16 || k < 1 || k_per_cta < 0)
+                {
+                        throw DError{NT_EINVAL, "nt_tc_gemm_bf16_t: bad arguments"};
+                }
+                cudaStream_t s = (cudaStream_t)stream;
+                Buf err;
+                err.ensure(sizeof(int));
+                ck(cudaMemsetAsync(err.p, 0, sizeof(int), s), "memset");
+                ck(cudaMemsetAsync(d_c, 0, (size_t)m * n * sizeof(float), s), "memset");
+                ck(gemm(LoadCols{(const __nv_bfloat16*)d_at, m}, LoadCols{(const __nv_bfloat16*)d_bt, n},
+                        EpiAtomicF32{d_c, n, n}, m, n, k, k_per_cta, err.as<int>(), s),
                    "gemm");
                 int h = 0;
                 ck(cudaMemcpyAsync(&h, err.p, sizeof(int), cudaMemcpyDeviceToHost, s), "copy");

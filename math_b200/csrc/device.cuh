@@ -357,8 +357,12 @@ __device__ __noinline__ Leaf<N> find_leaf_dfs(const MeshDev<N>& M, const Point<N
 }
 
 // Threads per block of every kernel that walks a tree: the path caches' per-level slots are laid
-// out in shared memory with this stride.
-constexpr int WALK_BLOCK = 256;
+// out in shared memory with this stride.  A build-time option (NT_BLOCK, with NT_WALK_MIN_BLOCKS the
+// occupancy asked of the walk kernels).
+#ifndef NT_BLOCK
+#define NT_BLOCK 256
+#endif
+constexpr int WALK_BLOCK = NT_BLOCK;
 
 // The root-to-leaf path of the previous point location of the same walk.  Consecutive leaves of a
 // walk share most of their ancestors; the child chosen at each level depends only on the point and
@@ -1672,7 +1676,7 @@ __device__ __forceinline__ int walk_step_warp(const MeshDev<N>& M, Walk<N>& w, b
 // order; the walk is needed unless a non-mesh object is strictly nearer than the mesh's root box
 // (then the loop breaks before the mesh).  pre: the choice made before the mesh entry; post: the
 // nearest non-mesh entry after it, compared with the walk's result.
-struct ClosestPlan
+struct __align__(16) ClosestPlan  // 32 bytes: two vector loads when stored in a walk list
 {
         int mesh_obj;        // object index of the mesh
         float mesh_t;        // its approximate distance (root box)

@@ -10,8 +10,7 @@ namespace ntrace
 {
 namespace
 {
-constexpr int BLOCK = 256;
-static_assert(BLOCK == WALK_BLOCK, "path-cache slots are laid out for the walk kernels' block size");
+constexpr int BLOCK = WALK_BLOCK;  // every wavefront kernel's block size
 // resident blocks per SM asked of the tree-walk kernels (caps their registers at 65536 / (2 x 256):
 // 2 blocks without spills measured faster than 3 or 4 with them)
 #ifndef NT_WALK_MIN_BLOCKS
@@ -701,13 +700,13 @@ __device__ __forceinline__ long long lane_refill(bool idle, unsigned long long* 
 }
 
 // Appends this lane's queue index to a walk list when `walk` (one atomic per warp; the lanes of a warp
-// keep their order).  Every lane of the warp calls it.
-__device__ __forceinline__ void list_append(bool walk, long long i, int* list, unsigned long long* count)
+// keep their order) and returns its list position (-1 without `walk`).  Every lane of the warp calls it.
+__device__ __forceinline__ long long list_append(bool walk, long long i, int* list, unsigned long long* count)
 {
         const unsigned m = __ballot_sync(0xffffffffu, walk);
         if (!m)
         {
-                return;
+                return -1;
         }
         const int lane = threadIdx.x & 31;
         const int leader = __ffs(m) - 1;
@@ -717,18 +716,24 @@ __device__ __forceinline__ void list_append(bool walk, long long i, int* list, u
                 base = atomicAdd(count, (unsigned long long)__popc(m));
         }
         base = __shfl_sync(0xffffffffu, base, leader);
-        if (walk)
+        if (!walk)
         {
-                list[base + __popc(m & lanemask_lt())] = (int)i;
+                return -1;
         }
+        const long long q = (long long)base + __popc(m & lanemask_lt());
+        list[q] = (int)i;
+        return q;
 }
+
+static_assert(sizeof(ClosestPlan) <= 32, "a listed ray's plan takes 32 bytes");
 
 // Extension rays of a scene with one mesh, first pass: every ray's objects (closest_plan); the rays
 // that need no tree walk are finished here (their hit record written), the others are compacted into
 // the walk list for k_extend_refill, so that its lanes only ever hold rays that walk.
 template <int N>
 __global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H,
-                                                       int* __restrict__ list, unsigned long long* counters)
+                                                       int* __restrict__ list, ClosestPlan* __restrict__ plans,
+                                                       unsigned long long* counters)
 {
         const long long count = (long long)counters[C_Q_ACTIVE];
         const int lane = threadIdx.x & 31;
@@ -739,6 +744,7 @@ __global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const D
         {
                 const long long i = w0 + lane;
                 bool walk = false;
+                ClosestPlan plan;
                 if (i < count)
                 {
                         ++rays;
@@ -749,7 +755,6 @@ __global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const D
                                 r.org[k] = A.at(k, i);
                                 r.dir[k] = A.at(N + k, i);
                         }
-                        ClosestPlan plan;
                         closest_plan<N>(S, r, &plan);
                         walk = plan.walk;
                         if (!walk)
@@ -766,7 +771,11 @@ __global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const D
                                 }
                         }
                 }
-                list_append(walk, i, list, counters + C_WALK_EXT);
+                const long long q = list_append(walk, i, list, counters + C_WALK_EXT);
+                if (q >= 0)
+                {
+                        plans[q] = plan;
+                }
         }
         warp_add(counters + C_RAYS, rays);
 }
@@ -776,7 +785,7 @@ __global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const D
 // its contribution here; the rest are compacted into the walk list for k_shadow_refill.
 template <int N>
 __global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ,
-                                                       double* accum, int* __restrict__ list,
+                                                       double* accum, int* __restrict__ list, float* __restrict__ entry,
                                                        unsigned long long* counters)
 {
         const long long count = (long long)counters[C_SHADOW];
@@ -788,6 +797,7 @@ __global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const D
         {
                 const long long j = w0 + lane;
                 bool walk = false;
+                float a_m = 0;
                 if (j < count)
                 {
                         ++rays;
@@ -810,6 +820,7 @@ __global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const D
                                 if (S.obj[o].kind == OBJ_MESH)
                                 {
                                         walk = true;
+                                        a_m = a;
                                 }
                                 else
                                 {
@@ -822,18 +833,22 @@ __global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const D
                                 accumulate(accum, SQ.pix[j], SQ.at(2 * N + 1, j), SQ.at(2 * N + 2, j), SQ.at(2 * N + 3, j));
                         }
                 }
-                list_append(walk, j, list, counters + C_WALK_SH);
+                const long long q = list_append(walk, j, list, counters + C_WALK_SH);
+                if (q >= 0)
+                {
+                        entry[q] = a_m;
+                }
         }
         warp_add(counters + C_SHADOW_RAYS, rays);
 }
 
-// Extension rays of a scene with one mesh that walk the tree (the plan kernel's list): closest_plan
-// again at fetch (cheap: slab tests), then one leaf per iteration.
+// Extension rays of a scene with one mesh that walk the tree (the plan kernel's list, with each ray's
+// closest_plan beside it), one leaf per iteration.
 // R: rounds of 32 pooled facet tests staged per warp chunk (Stage<N, R>).
 template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, const int* __restrict__ list,
-                        unsigned long long* counters)
+                        const ClosestPlan* __restrict__ plans, unsigned long long* counters)
 {
         const long long count = (long long)counters[C_WALK_EXT];
         const MeshDev<N>& M = S.mesh[0];
@@ -861,22 +876,9 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                                         r.org[k] = A.at(k, j);
                                         r.dir[k] = A.at(N + k, j);
                                 }
-                                closest_plan<N>(S, r, &plan);
-                                if (plan.walk)
-                                {
-                                        walk_begin<N>(w, r, plan.mesh_t, FLT_MAX);
-                                        i = j;
-                                }
-                                else if (plan.pre_obj >= 0)
-                                {
-                                        H.t[j] = plan.pre_t;
-                                        H.obj[j] = plan.pre_obj;
-                                        H.facet[j] = -1;
-                                }
-                                else
-                                {
-                                        H.obj[j] = -1;
-                                }
+                                plan = plans[q];  // listed rays have plan.walk set
+                                walk_begin<N>(w, r, plan.mesh_t, FLT_MAX);
+                                i = j;
                         }
                         if (exhausted || !__any_sync(0xffffffffu, i < 0))
                         {
@@ -917,12 +919,12 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         flush_stats<false>(counters, ws, rays, 0);
 }
 
-// Shadow rays of a scene with one mesh: a non-mesh object nearer than the light occludes at once;
-// otherwise the mesh is walked (up to the light's distance) when its root box starts before the light.
+// Shadow rays of a scene with one mesh that walk the tree (the plan kernel's list, with the distance
+// at which each ray enters the mesh's root box): the walk runs up to the light's distance.
 template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
         k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, const int* __restrict__ list,
-                        unsigned long long* counters)
+                        const float* __restrict__ entry, unsigned long long* counters)
 {
         const long long count = (long long)counters[C_WALK_SH];
         const MeshDev<N>& M = S.mesh[0];
@@ -940,7 +942,6 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                         const long long q = lane_refill(i < 0, counters + C_WORK_SH, count, &exhausted);
                         if (q >= 0)
                         {
-                                // a listed ray walks (k_plan_shadow); its mesh's entry distance again here
                                 const long long j = list[q];
                                 Ray<N> r;
 #pragma unroll
@@ -949,41 +950,12 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
                                         r.org[k] = SQ.at(k, j);
                                         r.dir[k] = SQ.at(N + k, j);
                                 }
-                                float dj = SQ.at(2 * N, j);
-                                bool occluded = false;
-                                bool walk = false;
-                                float a_m = 0;
-                                for (int o = 0; o < S.nobj; ++o)
-                                {
-                                        float a;
-                                        if (!obj_approx<N>(S, o, r, &a) || !(a < dj))
-                                        {
-                                                continue;
-                                        }
-                                        if (S.obj[o].kind == OBJ_MESH)
-                                        {
-                                                walk = true;
-                                                a_m = a;
-                                        }
-                                        else
-                                        {
-                                                occluded = true;
-                                        }
-                                }
-                                if (!occluded)
-                                {
-                                        if (walk)
-                                        {
-                                                walk_begin<N>(w, r, a_m, dj);
-                                                dist = dj;
-                                                i = j;
-                                        }
-                                        else
-                                        {
-                                                accumulate(accum, SQ.pix[j], SQ.at(2 * N + 1, j), SQ.at(2 * N + 2, j),
-                                                           SQ.at(2 * N + 3, j));
-                                        }
-                                }
+                                // listed by k_plan_shadow: nothing nearer than the light occludes it, and the
+                                // mesh's root box starts before the light at entry[q]
+                                const float dj = SQ.at(2 * N, j);
+                                walk_begin<N>(w, r, entry[q], dj);
+                                dist = dj;
+                                i = j;
                         }
                         if (exhausted || !__any_sync(0xffffffffu, i < 0))
                         {
@@ -1241,8 +1213,9 @@ size_t Wavefront<N>::bytes_for(long long Q, int lights, bool smooth)
                           + sizeof(uint32_t) * 2 * 2 + sizeof(int) * 2
                           + sizeof(float) + sizeof(int) * 2  // hit record
                           + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights * (smooth ? 2 : 1)  // shadow queues
-                          + sizeof(int) * (1 + (size_t)lights);  // walk lists
-        return per_path * (size_t)Q + 20 * 256;
+                          + sizeof(int) * (1 + (size_t)lights)  // walk lists
+                          + 32 + sizeof(float) * (size_t)lights;  // the plans of the listed rays
+        return per_path * (size_t)Q + 22 * 256;
 }
 
 template <int N>
@@ -1270,6 +1243,8 @@ void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
         sq_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
         walk_ext = (int*)take(sizeof(int) * Q);
         walk_sh = (int*)take(sizeof(int) * Q * lights);
+        plan_ext = take(32 * Q);
+        plan_sh = (float*)take(sizeof(float) * Q * lights);
         if (smooth)
         {
                 sm_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
@@ -1355,7 +1330,7 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         if (one_mesh)
         {
                 // rays that need no walk are finished by the plan kernel; the walk kernel takes the rest
-                k_plan_extend<N><<<str_grid, BLOCK, 0, st>>>(S, A, H, walk_ext, counters);
+                k_plan_extend<N><<<str_grid, BLOCK, 0, st>>>(S, A, H, walk_ext, (ClosestPlan*)plan_ext, counters);
         }
         if (ev)
         {
@@ -1365,19 +1340,19 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         {
                 if (vi == 0)
                 {
-                        k_extend_refill<N, 0><<<ext_grid, BLOCK, 0, st>>>(S, A, H, walk_ext, counters);
+                        k_extend_refill<N, 0><<<ext_grid, BLOCK, 0, st>>>(S, A, H, walk_ext, (const ClosestPlan*)plan_ext, counters);
                 }
                 else if (vi == 1)
                 {
-                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, walk_ext, counters);
+                        k_extend_refill<N, 1><<<ext_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, A, H, walk_ext, (const ClosestPlan*)plan_ext, counters);
                 }
                 else if (vi == 2)
                 {
-                        k_extend_refill<N, 2><<<ext_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, A, H, walk_ext, counters);
+                        k_extend_refill<N, 2><<<ext_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, A, H, walk_ext, (const ClosestPlan*)plan_ext, counters);
                 }
                 else
                 {
-                        k_extend_refill<N, 4><<<ext_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, A, H, walk_ext, counters);
+                        k_extend_refill<N, 4><<<ext_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, A, H, walk_ext, (const ClosestPlan*)plan_ext, counters);
                 }
         }
         else
@@ -1395,7 +1370,7 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         }
         if (one_mesh)
         {
-                k_plan_shadow<N><<<str_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, counters);
+                k_plan_shadow<N><<<str_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
         }
         if (ev)
         {
@@ -1405,19 +1380,19 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         {
                 if (vi == 0)
                 {
-                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, counters);
+                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
                 }
                 else if (vi == 1)
                 {
-                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, walk_sh, counters);
+                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
                 }
                 else if (vi == 2)
                 {
-                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, walk_sh, counters);
+                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
                 }
                 else
                 {
-                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, walk_sh, counters);
+                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
                 }
         }
         else

@@ -55,9 +55,13 @@ struct Wavefront
         int* hit_facet = nullptr;
         float* sq_f = nullptr;
         uint32_t* sq_pix = nullptr;
-        // one-mesh scenes: queue indices of the extension and shadow rays that walk the tree
+        // one-mesh scenes: queue indices of the extension and shadow rays that walk the tree, and what
+        // the plan kernels found for them (the extension rays' object plan, 32 bytes each; the shadow
+        // rays' mesh entry distance), so that the walk kernels do not work it out again
         int* walk_ext = nullptr;
         int* walk_sh = nullptr;
+        void* plan_ext = nullptr;
+        float* plan_sh = nullptr;
         // smooth-normal shadow queue (only when some mesh has vertex normals and smooth_normal is set)
         float* sm_f = nullptr;
         uint32_t* sm_pix = nullptr;

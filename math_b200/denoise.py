@@ -51,6 +51,7 @@ def _lib() -> ctypes.CDLL:
             "nt_denoiser_train_step": ([vp, vp, ctypes.c_float, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
             "nt_tc_gemm_bf16": ([vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
             "nt_tc_gemm_wait_selftest": ([vp], ctypes.c_int),
+            "nt_tc_gemm_bf16_t": ([vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp], ctypes.c_int),
         }
         for name, (args, res) in sig.items():
             fn = getattr(lib, name)
@@ -83,6 +84,25 @@ def tc_gemm(a, b):
     c = torch.empty((m, n), dtype=torch.float32, device=a.device)
     _check(_lib().nt_tc_gemm_bf16(a.data_ptr(), b.data_ptr(), c.data_ptr(), m, n, k,
                                   torch.cuda.current_stream().cuda_stream or None))
+    return c
+
+
+def tc_gemm_t(at, bt, k_per_cta: int = 0):
+    """C = At^T Bt on the tensor cores, the weight-gradient form: At (k x m) and Bt (k x n) bfloat16
+    CUDA tensors read transposed; the k range split over CTAs of k_per_cta (0: not split); C float32."""
+    import torch
+
+    if at.dtype != torch.bfloat16 or bt.dtype != torch.bfloat16 or not (at.is_cuda and bt.is_cuda):
+        raise ValueError("expected bfloat16 CUDA tensors")
+    at = at.contiguous()
+    bt = bt.contiguous()
+    k, m = at.shape
+    k2, n = bt.shape
+    if k != k2:
+        raise ValueError("inner dimensions differ")
+    c = torch.empty((m, n), dtype=torch.float32, device=at.device)
+    _check(_lib().nt_tc_gemm_bf16_t(at.data_ptr(), bt.data_ptr(), c.data_ptr(), m, n, k, k_per_cta,
+                                    torch.cuda.current_stream().cuda_stream or None))
     return c
 
 
@@ -370,6 +390,6 @@ def spp_for_rmse(rmse_at_spp: float, spp: int, target: float) -> float:
     return spp * (rmse_at_spp / target) ** 2 if rmse_at_spp > 0 else spp
 
 
-__all__ = ["Denoiser", "Layout", "tc_gemm", "relative_rmse", "screen_axes", "random_variant", "apply_variant",
+__all__ = ["Denoiser", "Layout", "tc_gemm", "tc_gemm_t", "relative_rmse", "screen_axes", "random_variant", "apply_variant",
            "render_inputs", "render_reference", "make_pairs", "set_pair", "train", "evaluate",
            "uniform_filter_params", "time_call", "spp_for_rmse", "NtraceError"]

@@ -40,7 +40,7 @@ EXPORTED_SYMBOLS = (
     "nt_render_moments", "nt_render_noalloc", "nt_render_pixels", "nt_probe_peaks",
     "nt_denoiser_create", "nt_denoiser_destroy", "nt_denoiser_get_layout", "nt_denoiser_get_params",
     "nt_denoiser_set_params", "nt_denoiser_set_input", "nt_denoiser_apply", "nt_denoiser_gradient",
-    "nt_denoiser_train_step", "nt_tc_gemm_bf16", "nt_tc_gemm_wait_selftest",
+    "nt_denoiser_train_step", "nt_tc_gemm_bf16", "nt_tc_gemm_bf16_t", "nt_tc_gemm_wait_selftest",
 )
 
 

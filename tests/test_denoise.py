@@ -183,6 +183,24 @@ def test_tc_gemm_matches_torch(require_gpu, m, n, k):
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("m,n,k,kpc", [(8, 16, 16, 0), (64, 64, 4096, 1024), (144, 64, 3000, 512),
+                                       (136, 48, 200, 0), (128, 256, 130, 64)])
+def test_tc_gemm_transposed_split_matches_torch(require_gpu, m, n, k, kpc):
+    """The weight-gradient form: both operands read MN-major (transposed row-major matrices), ragged
+    k, and the k range split over CTAs with FP32 atomics."""
+    torch = _torch()
+    from math_b200.denoise import tc_gemm_t
+
+    g = torch.Generator(device="cpu").manual_seed(m + 3 * n + k)
+    at = torch.randn(k, m, generator=g).to(torch.bfloat16).cuda()
+    bt = torch.randn(k, n, generator=g).to(torch.bfloat16).cuda()
+    c = tc_gemm_t(at, bt, kpc)
+    ref = at.float().T @ bt.float()
+    err = (c - ref).abs().max().item()
+    assert err <= 1e-3 * max(1.0, ref.abs().max().item()), err
+
+
+@pytest.mark.gpu
 def test_tc_gemm_wait_runs_out_and_reports(require_gpu):
     """Failure detection without a fault: the GEMM kernel with its tensor-core instructions withheld
     (nothing ever arrives on its barrier) gives up its bounded wait, frees its tensor memory and reports
