@@ -371,15 +371,13 @@ constexpr int WALK_BLOCK = NT_BLOCK;
 struct PathCache
 {
         int depth;                 // level of the cached leaf; -1: empty
-        unsigned long long bits;   // child index chosen at each level, 6 bits per level
         int2 leaf;                 // the cached leaf's record
-        // the first child of the internal node at each level of the path is kept in shared memory
-        // (path_cache_slots)
+        // the first child of the internal node at each level of the path, and the child chosen there,
+        // are kept in shared memory (path_cache_slots, path_cache_child)
 
         __device__ __forceinline__ void reset()
         {
                 depth = -1;
-                bits = 0;
         }
 };
 
@@ -390,11 +388,20 @@ __device__ __forceinline__ int* path_cache_slots()
         return s_fc + threadIdx.x;
 }
 
+// This thread's column of the child indices chosen along the cached path (MAX_LEVELS x WALK_BLOCK
+// bytes; consecutive threads share 32-bit words, which costs no bank conflicts).
+__device__ __forceinline__ unsigned char* path_cache_child()
+{
+        __shared__ unsigned char s_child[MAX_LEVELS * WALK_BLOCK];
+        return s_child + threadIdx.x;
+}
+
 template <int N>
 __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const float* p, PathCache& pc, Leaf<N>* out,
                                                  int2* leaf_rec, unsigned* descent)
 {
         int* const fc = path_cache_slots();
+        unsigned char* const cc = path_cache_child();
 #pragma unroll
         for (int i = 0; i < N; ++i)
         {
@@ -485,12 +492,11 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                         }
                         return false;
                 }
-                const int shift = 6 * lvl;
-                if (same && (int)((pc.bits >> shift) & 63ull) != child)
+                if (!same || (int)cc[lvl * WALK_BLOCK] != child)
                 {
                         same = false;
+                        cc[lvl * WALK_BLOCK] = (unsigned char)child;
                 }
-                pc.bits = (pc.bits & ~(63ull << shift)) | ((unsigned long long)child << shift);
                 node = nd.x + child;
         }
         pc.depth = -1;

@@ -335,8 +335,10 @@ def set_pair(den: Denoiser, pair: dict) -> None:
     den.set_input(pair["screen"], pair["mean"], pair["var"], pair["normal"], pair["depth"], pair["spp"])
 
 
-def train(den: Denoiser, pairs: list[dict], steps: int, lr: float = 1e-3, seed: int = 0, log=None) -> list[float]:
-    """Adam steps over the pairs in a seeded shuffled order; returns the loss of every step."""
+def train(den: Denoiser, pairs: list[dict], steps: int, lr: float = 1e-3, seed: int = 0, log=None,
+          lr_final: float | None = None) -> list[float]:
+    """Adam steps over the pairs in a seeded shuffled order; returns the loss of every step.  The
+    learning rate is lr throughout, or with lr_final it falls from lr to lr_final along a half cosine."""
     rng = np.random.default_rng(seed)
     losses = []
     order = []
@@ -345,7 +347,8 @@ def train(den: Denoiser, pairs: list[dict], steps: int, lr: float = 1e-3, seed: 
             order = list(rng.permutation(len(pairs)))
         p = pairs[order.pop()]
         set_pair(den, p)
-        losses.append(den.train_step(p["target"], lr))
+        rate = lr if lr_final is None else lr_final + 0.5 * (lr - lr_final) * (1.0 + np.cos(np.pi * s / max(1, steps)))
+        losses.append(den.train_step(p["target"], rate))
         if log and (s % 100 == 0 or s == steps - 1):
             log(f"step {s} loss {losses[-1]:.5f}")
     return losses

@@ -191,6 +191,8 @@ def main(argv=None) -> None:
     ap.add_argument("--pairs", type=int, default=200)
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--lr", type=float, default=1e-3)
+    ap.add_argument("--lr-final", type=float, default=None,
+                    help="fall from --lr to this along a half cosine over the steps (default: constant --lr)")
     ap.add_argument("--k-in", type=int, nargs="+", default=[1, 2, 3, 4, 6, 8],
                     help="input samples per pixel of the training pairs: k^(n-1) for k drawn from these "
                          "(those with k^(n-1) above spp-ref / 16 are left out)")
@@ -216,7 +218,8 @@ def main(argv=None) -> None:
         scene = scenes.build_scene(spec, tree_on_gpu=True)
         build_s = time.perf_counter() - t0
         path = out / f"denoiser_n{n}.npz"
-        report = {"n": n, "scene_build_seconds": build_s, "k_in": k_in}
+        report = {"n": n, "scene_build_seconds": build_s, "k_in": k_in, "pairs": args.pairs, "steps": args.steps,
+                  "lr": args.lr, "lr_final": args.lr_final}
         if args.load:
             den = denoise.Denoiser.load(path)
         else:
@@ -229,7 +232,7 @@ def main(argv=None) -> None:
             uni = denoise.Denoiser(n, seed=args.seed)
             uni.set_params(denoise.uniform_filter_params(uni))
             t0 = time.perf_counter()
-            losses = denoise.train(den, pairs, args.steps, args.lr, seed=args.seed)
+            losses = denoise.train(den, pairs, args.steps, args.lr, seed=args.seed, lr_final=args.lr_final)
             report["train_seconds"] = time.perf_counter() - t0
             report["loss_first_100"] = float(np.mean(losses[:100]))
             report["loss_last_100"] = float(np.mean(losses[-100:]))
