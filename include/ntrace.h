@@ -59,6 +59,10 @@ typedef struct nt_build_opts
                           without a GPU; render and trace calls then fail with NT_ESTATE) */
         int tree_on_gpu; /* 1: build the 2^n-trees on the GPU (the same trees, box for box, as the host
                             build; much faster for large meshes and for n >= 5); ignored with host_only */
+        int leaf_records; /* 0: keep a copy of the FP32 facet records in leaf-list order (a facet's record
+                             once per leaf that lists it) when it takes at most a quarter of the free
+                             device memory, so that a leaf's records are read without its index list;
+                             -1: never (records read through the index lists).  Same results either way. */
 } nt_build_opts;
 
 typedef struct nt_render_opts

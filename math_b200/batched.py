@@ -31,6 +31,8 @@ from . import ntrace, scenes
 # n = 6, 5e3 points, 0.78 M facets: 59 s; the facet count per point grows steeply with n, so a 2e5-point
 # hull at n = 6 would hold some 2e7 facets and take hours).
 POINT_RANGE = {3: (1_000, 200_000), 4: (1_000, 200_000), 5: (1_000, 50_000), 6: (1_000, 3_000)}
+# path pool per scene at most (the batch's pools are resident together)
+MAX_POOL = 16 << 20
 # screens from 64^2 (n = 3) up to 32^5 (n = 6) pixels
 SCREEN_RANGE = {3: (64, 512), 4: (32, 128), 5: (16, 48), 6: (8, 32)}
 
@@ -89,7 +91,10 @@ def run(count: int = 64, seed: int = 0, repeat: int = 3, cache: Path | None = No
     t0 = time.perf_counter()
     specs = make_workload(count, seed, cache, max_points)
     mesh_s = time.perf_counter() - t0
-    built = [scenes.build_scene(sp, tree_on_gpu=True) for sp in specs]
+    # the 64 scenes stay resident together, so their meshes keep only the compact record arrays (no
+    # leaf-ordered copy, which repeats a record once per leaf listing it: several GB for the larger n = 5
+    # and 6 hulls), and their path pools are capped at MAX_POOL paths
+    built = [scenes.build_scene(sp, tree_on_gpu=True, leaf_records=-1) for sp in specs]
     build_s = time.perf_counter() - t0
     # autotune once per dimension on its largest scene; apply to every scene of that dimension
     tuned = {}
@@ -103,7 +108,8 @@ def run(count: int = 64, seed: int = 0, repeat: int = 3, cache: Path | None = No
     opts = []
     for sp in specs:
         t = tuned[sp["n"]]
-        opts.append(dict(samples_per_pixel=sp["spp"], max_depth=5, seed=sp["seed"], pool_paths=t["pool_paths"],
+        opts.append(dict(samples_per_pixel=sp["spp"], max_depth=5, seed=sp["seed"],
+                         pool_paths=min(t["pool_paths"], MAX_POOL),
                          graph_iterations=t["graph_iterations"], walk_chunk=t["walk_chunk"],
                          walk_small_leaf=t["walk_small_leaf"]))
     paths = sum(s.pixel_count * ntrace.effective_spp(sp["n"], sp["spp"]) for s, sp in zip(built, specs))
@@ -126,6 +132,7 @@ def run(count: int = 64, seed: int = 0, repeat: int = 3, cache: Path | None = No
         "batch_paths_per_s": paths / batch_s, "sequential_paths_per_s": paths / seq_s, "batch_seconds": batch_s,
         "sequential_seconds": seq_s, "tuned": {str(k): v for k, v in tuned.items()},
         "facets": [int(len(sp["facets"])) for sp in specs], "points": [sp["points"] for sp in specs],
+        "mesh_device_bytes": [int(s.mesh_info(0)["device_bytes"]) for s in built],
         "screens": [sp["projector"]["screen"][0] for sp in specs], "dims": [sp["n"] for sp in specs],
     }
     for sc in built:

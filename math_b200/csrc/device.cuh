@@ -396,12 +396,47 @@ __device__ __forceinline__ unsigned char* path_cache_child()
         return s_child + threadIdx.x;
 }
 
+// Resumable descents.  The descent's choice at a level depends only on the point and the box origin
+// there, so a point that makes, at every level above L, the choice the cached path made there, without
+// a tie, meets the cached path's node and origin at level L and may start there.  Per axis those
+// choices hold exactly when lo < p < hi, where lo is the origin at level L along the axis if the path
+// took the upper half there at some level above L (the origin only grows, and it is set to the mid
+// point each time; otherwise no bound beyond the root box's), and hi the least of the mid points where
+// it took the lower half (p < mid: no tie) and of the just-above-upper-bounds where it took the upper
+// one (p <= mid + h).  Each internal level a descent passes leaves its origin, bound hi and upper-half
+// mask (the state before its own choice) in one of two slots per thread (slot = level mod 2, tagged
+// with the level), so the parent and grandparent of the cached leaf can be tried first; a slot whose tag
+// matches was written on the cached path (a descent rewrites every level it passes, and the levels
+// above its start are those it shares with the path before).  Above n = 4 only the parent's slot is
+// kept (slot 0).
+template <int N>
+struct DescentSlots
+{
+        // slots per thread: parent and grandparent up to n = 4, the parent alone above (the walk
+        // kernels' static shared memory stays within 48 KB)
+        static constexpr int K = N <= 4 ? 2 : 1;
+        float* o;    // [K][N][WALK_BLOCK]
+        float* hi;   // [K][N][WALK_BLOCK]
+        int* tag;    // [K][WALK_BLOCK]: level | upper-half mask << 8
+};
+
+template <int N>
+__device__ __forceinline__ DescentSlots<N> descent_slots()
+{
+        constexpr int K = DescentSlots<N>::K;
+        __shared__ float s_o[K * N * WALK_BLOCK];
+        __shared__ float s_hi[K * N * WALK_BLOCK];
+        __shared__ int s_tag[K * WALK_BLOCK];
+        return DescentSlots<N>{s_o + threadIdx.x, s_hi + threadIdx.x, s_tag + threadIdx.x};
+}
+
 template <int N>
 __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const float* p, PathCache& pc, Leaf<N>* out,
                                                  int2* leaf_rec, unsigned* descent)
 {
         int* const fc = path_cache_slots();
         unsigned char* const cc = path_cache_child();
+        const DescentSlots<N> ds = descent_slots<N>();
 #pragma unroll
         for (int i = 0; i < N; ++i)
         {
@@ -410,16 +445,60 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                         return false;
                 }
         }
-        float o[N];
+        float o[N], hi[N];
 #pragma unroll
         for (int i = 0; i < N; ++i)
         {
                 o[i] = M.root_org[i];
+                hi[i] = INFINITY;
         }
         int node = 0;
+        int upper = 0;  // axes along which the path took the upper half at some level above
+        int start = 0;
+        // the cached leaf's parent, then its grandparent
+        constexpr int K = DescentSlots<N>::K;
+        for (int back = 1; back <= K; ++back)
+        {
+                const int L = pc.depth - back;
+                if (L < 1)
+                {
+                        break;
+                }
+                const int slot = L % K;
+                const int tag = ds.tag[slot * WALK_BLOCK];
+                if ((tag & 255) != L)
+                {
+                        continue;
+                }
+                const int up = tag >> 8;
+                bool in = true;
+#pragma unroll
+                for (int i = 0; i < N; ++i)
+                {
+                        const float so = ds.o[(slot * N + i) * WALK_BLOCK];
+                        const float sh = ds.hi[(slot * N + i) * WALK_BLOCK];
+                        in = in && p[i] < sh && (((up >> i) & 1) == 0 || p[i] > so);
+                }
+                if (in)
+                {
+#pragma unroll
+                        for (int i = 0; i < N; ++i)
+                        {
+                                o[i] = ds.o[(slot * N + i) * WALK_BLOCK];
+                                hi[i] = ds.hi[(slot * N + i) * WALK_BLOCK];
+                        }
+                        upper = up;
+                        node = fc[(L - 1) * WALK_BLOCK] + (int)cc[(L - 1) * WALK_BLOCK];
+                        start = L;
+                        break;
+                }
+        }
+        // the levels above the start count as levels of the descent (the work counters describe the
+        // full descent from the root)
+        *descent += (unsigned)start;
         bool ambiguous = false;
         bool same = pc.depth >= 0;
-        for (int lvl = 0; lvl < MAX_LEVELS; ++lvl)
+        for (int lvl = start; lvl < MAX_LEVELS; ++lvl)
         {
                 int2 nd;
                 if (same)
@@ -449,6 +528,16 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                 {
                         fc[lvl * WALK_BLOCK] = nd.x;
                 }
+                {
+                        const int slot = lvl % K;
+                        ds.tag[slot * WALK_BLOCK] = lvl | (upper << 8);
+#pragma unroll
+                        for (int i = 0; i < N; ++i)
+                        {
+                                ds.o[(slot * N + i) * WALK_BLOCK] = o[i];
+                                ds.hi[(slot * N + i) * WALK_BLOCK] = hi[i];
+                        }
+                }
                 int child = 0;
                 bool fail = false;
 #pragma unroll
@@ -456,22 +545,26 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                 {
                         float h = M.size[lvl + 1][i];
                         float mid = o[i] + h;
+                        float top = mid + h;
                         bool lo_ok = p[i] <= mid;
-                        bool hi_ok = (-p[i] <= -mid) && (p[i] <= mid + h);
+                        bool hi_ok = (-p[i] <= -mid) && (p[i] <= top);
                         if (lo_ok)
                         {
                                 ambiguous |= hi_ok;
+                                hi[i] = fminf(hi[i], mid);
                         }
                         else if (hi_ok)
                         {
                                 child |= 1 << i;
                                 o[i] = mid;
+                                hi[i] = fminf(hi[i], nextafterf(top, INFINITY));
                         }
                         else
                         {
                                 fail = true;
                         }
                 }
+                upper |= child;
                 if (fail)
                 {
                         pc.depth = -1;
@@ -744,6 +837,16 @@ __device__ __noinline__ double retest_facet(const double* rec, const Ray<N> ray,
 
 // Closest facet of one leaf (ray_intersection over indices, ray_intersection.h:134-159: strict <
 // in list order).  Returns the facet or -1 and its distance.
+// The FP32 record of leaf-list entry pos: from the leaf-ordered copy when the mesh has one, else
+// through the leaf's index list (the copy is left out when it would take more than a quarter of the
+// free device memory; the branch is uniform, on a kernel parameter).
+template <int N>
+__device__ __forceinline__ const float4* leaf_record(const MeshDev<N>& M, long long pos)
+{
+        return M.leaf_rec32 ? M.leaf_rec32 + (size_t)pos * Rec32<N>::F4
+                            : M.rec32 + (size_t)__ldg(&M.leaf_idx[pos]) * Rec32<N>::F4;
+}
+
 template <int N>
 __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, const Ray<N>& ray, float ao,
                                             const Ray64Source<N>& src, int retest, float* t_best, WalkStats* ws)
@@ -756,7 +859,7 @@ __device__ __forceinline__ int leaf_closest(const MeshDev<N>& M, int2 leaf, cons
         {
                 ++ws->facet_tests;
                 float t;
-                int res = facet_test32<N>(M.leaf_rec32 + (size_t)(leaf.x + q) * Rec32<N>::F4, ray, ao, &t);
+                int res = facet_test32<N>(leaf_record<N>(M, leaf.x + q), ray, ao, &t);
                 if (res == T_MISS)
                 {
                         continue;
@@ -1275,7 +1378,7 @@ __device__ __forceinline__ void walk_begin(Walk<N>& w, const Ray<N>& ray, float 
 // then reads its own slots in leaf-list order and makes the same sequential choice as leaf_closest
 // (strict < in list order, near-ties settled in FP64), so the result is the per-lane loop's.
 
-constexpr int POOL_SLOTS = 128;  // pooled tests per warp and round
+constexpr int POOL_SLOTS = 128;  // pooled tests per warp and round, at most
 constexpr int SMALL_LEAF = 2;  // default: leaves this small are tested per lane, not pooled
 
 struct PoolSlot
@@ -1285,10 +1388,12 @@ struct PoolSlot
         double t64;   // FP64 distance when re-tested; -1 otherwise
 };
 
+// The warp's outcome slots, SLOTS of them (a kernel variant's chunk size: 32 to POOL_SLOTS).
+template <int SLOTS>
 __device__ __forceinline__ PoolSlot* warp_pool()
 {
-        __shared__ PoolSlot s_pool[(WALK_BLOCK / 32) * POOL_SLOTS];
-        return s_pool + (threadIdx.x >> 5) * POOL_SLOTS;
+        __shared__ PoolSlot s_pool[(WALK_BLOCK / 32) * SLOTS];
+        return s_pool + (threadIdx.x >> 5) * SLOTS;
 }
 
 // Facet records staged through shared memory.  A warp handles its pooled tests in chunks of
@@ -1375,7 +1480,7 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                 *t_best = bt;
                 return best;
         }
-        PoolSlot* pool = warp_pool();
+        PoolSlot* pool = warp_pool<Stage<N, RR>::SLOTS>();
         constexpr bool STAGED = RR > 0;
         constexpr int R = Stage<N, RR>::ROUNDS;
         constexpr int F4 = Rec32<N>::F4;
@@ -1416,7 +1521,7 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                         {
                                 if (pos[r] >= 0)
                                 {
-                                        const float4* src = M.leaf_rec32 + (size_t)pos[r] * F4;
+                                        const float4* src = leaf_record<N>(M, pos[r]);
                                         float4* dst = stage + (size_t)(32 * r + lane) * F4;
 #pragma unroll
                                         for (int q = 0; q < F4; ++q)
@@ -1448,7 +1553,7 @@ __device__ __forceinline__ int leaf_closest_warp(const MeshDev<N>& M, int start,
                                 double t64 = -1.0;
                                 int keep = -1;
                                 int res = STAGED ? facet_test32<N, true>(stage + (size_t)(32 * r + lane) * F4, rr, o_ao, &t)
-                                                 : facet_test32<N, false>(M.leaf_rec32 + (size_t)pos[r] * F4, rr, o_ao, &t);
+                                                 : facet_test32<N, false>(leaf_record<N>(M, pos[r]), rr, o_ao, &t);
                                 const int f = res != T_MISS ? __ldg(&M.leaf_idx[pos[r]]) : -1;
                                 if (res == T_HIT)
                                 {

@@ -57,7 +57,8 @@ struct MeshDev
         const int2* nodes;     // internal: {first_child, -1}; leaf: {index offset, count}
         const int* leaf_idx;
         const float4* leaf_rec32;  // the leaves' FP32 records in leaf-list order (rec32 gathered through
-                                   // leaf_idx): a leaf's records are read without its index list first
+                                   // leaf_idx): a leaf's records are read without its index list first;
+                                   // null when the copy did not fit the memory budget (leaf_record)
         // vertex normals (null without them): normals (count x N), per-facet normal indices (N per
         // facet) and per-facet NormalType: 0 None, 1 Use, 2 Reverse with bit 2 + i set when vertex i's
         // normal is reversed (mesh_hyperplane_simplex.cpp:96-143)

@@ -322,6 +322,7 @@ struct nt_scene
         nt_surface background{{0, 0, 0}, 1, 0, {0, 0, 0}};
         bool built = false;       // built and uploaded: renderable
         bool built_host = false;  // facet setup and trees built on the host only
+        int leaf_records = 0;     // nt_build_opts.leaf_records
         float ray_offset = 0;
         // device
         cudaStream_t stream = nullptr;
@@ -946,13 +947,28 @@ int rec32_f4(int n)
 }
 
 // The leaves' records in leaf-list order, gathered on the device from the uploaded record and index
-// arrays (after every upload of those, on the scene's stream).
-void gather_leaf_records(MeshHost& m, int n, cudaStream_t st)
+// arrays (after every upload of those, on the scene's stream).  The copy repeats a facet's record in
+// every leaf that lists it (about 50 times at n = 4), so it is made only while it takes at most a
+// quarter of the free device memory; without it the kernels read a leaf's records through its index
+// list (leaf_record), with the same results.
+void gather_leaf_records(MeshHost& m, int n, cudaStream_t st, int policy)
 {
         const long long count = (long long)(m.d_idx.bytes / sizeof(int32_t));
         const size_t bytes = std::max<size_t>((size_t)count * rec32_f4(n) * 16, 16);
+        if (policy < 0)
+        {
+                m.d_leafrec.reset();
+                return;
+        }
         if (m.d_leafrec.bytes != bytes)
         {
+                m.d_leafrec.reset();
+                size_t free_b = 0, total_b = 0;
+                check_cuda(cudaMemGetInfo(&free_b, &total_b), "memory info");
+                if (bytes > free_b / 4)
+                {
+                        return;
+                }
                 m.d_leafrec.alloc(bytes);
         }
         check_cuda(launch_gather_records(m.d_rec32.as<float4>(), m.d_idx.as<int>(), count, rec32_f4(n),
@@ -1045,7 +1061,7 @@ void build_scene(nt_scene* s, unsigned threads, bool host_only, bool tree_on_gpu
                         m.d_rec64.upload(m.rec64, s->stream);
                         m.d_nodes.upload(m.nodes, s->stream);
                         m.d_idx.upload(m.leaf_idx, s->stream);
-                        gather_leaf_records(m, N, s->stream);
+                        gather_leaf_records(m, N, s->stream, s->leaf_records);
                         if (!m.ntype.empty())
                         {
                                 m.d_normals.upload(m.normals, s->stream);
@@ -2142,6 +2158,7 @@ int nt_scene_build(nt_scene* scene, const nt_build_opts* opts)
                 unsigned threads = (opts && opts->threads > 0) ? (unsigned)opts->threads : hardware_threads();
                 bool host_only = opts && opts->host_only;
                 bool tree_on_gpu = opts && opts->tree_on_gpu;
+                scene->leaf_records = opts ? opts->leaf_records : 0;
                 scene->built = false;
                 scene->built_host = false;
                 // an upload staged before the build is of the old scene: a commit now is refused
@@ -2239,7 +2256,7 @@ int nt_scene_upload(nt_scene* scene, int64_t* bytes)
                                 p += b->bytes;
                                 total += (int64_t)b->bytes;
                         }
-                        gather_leaf_records(m, scene->n, scene->stream);
+                        gather_leaf_records(m, scene->n, scene->stream, scene->leaf_records);
                 }
                 check_cuda(cudaStreamSynchronize(scene->stream), "upload sync");
                 if (bytes)
@@ -2323,7 +2340,7 @@ int nt_scene_upload_commit(nt_scene* scene)
                 // the leaf-ordered records are made from the live arrays, after the staging buffer is free
                 for (auto& m : scene->meshes)
                 {
-                        gather_leaf_records(m, scene->n, scene->stream);
+                        gather_leaf_records(m, scene->n, scene->stream, scene->leaf_records);
                 }
                 scene->consumed_recorded = true;
                 scene->upload_staged = false;

@@ -56,7 +56,8 @@ class Surface(ctypes.Structure):
 
 
 class BuildOpts(ctypes.Structure):
-    _fields_ = [("threads", ctypes.c_int), ("host_only", ctypes.c_int), ("tree_on_gpu", ctypes.c_int)]
+    _fields_ = [("threads", ctypes.c_int), ("host_only", ctypes.c_int), ("tree_on_gpu", ctypes.c_int),
+                ("leaf_records", ctypes.c_int)]
 
 
 class RenderOpts(ctypes.Structure):
@@ -319,9 +320,12 @@ class Scene:
         s = _surface(color, 1.0, light_source, light_color)
         _check(self._lib.nt_scene_set_background(self._h, ctypes.byref(s)))
 
-    def build(self, threads: int = 0, host_only: bool = False, tree_on_gpu: bool = False) -> None:
-        """Facet setup and 2^n-trees (on the GPU with tree_on_gpu), then the upload."""
-        o = BuildOpts(threads, int(bool(host_only)), int(bool(tree_on_gpu)))
+    def build(self, threads: int = 0, host_only: bool = False, tree_on_gpu: bool = False,
+              leaf_records: int = 0) -> None:
+        """Facet setup and 2^n-trees (on the GPU with tree_on_gpu), then the upload.  leaf_records: 0 keeps
+        the leaf-ordered copy of the facet records when it fits a quarter of the free device memory,
+        -1 never (nt_build_opts.leaf_records)."""
+        o = BuildOpts(threads, int(bool(host_only)), int(bool(tree_on_gpu)), int(leaf_records))
         _check(self._lib.nt_scene_build(self._h, ctypes.byref(o)))
 
     # ---- queries ----

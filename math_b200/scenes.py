@@ -220,7 +220,7 @@ def effective_spp(n: int, spp: int) -> int:
     return f ** m if f ** m >= spp else math.ceil(v) ** m
 
 
-def build_scene(spec: dict, threads: int = 0, tree_on_gpu: bool = False) -> ntrace.Scene:
+def build_scene(spec: dict, threads: int = 0, tree_on_gpu: bool = False, leaf_records: int = 0) -> ntrace.Scene:
     n = spec["n"]
     s = ntrace.Scene(n)
     if spec["verts"] is not None:
@@ -245,5 +245,5 @@ def build_scene(spec: dict, threads: int = 0, tree_on_gpu: bool = False) -> ntra
     s.set_projector(P["kind"], P["org"], P["dir"], P["axes"], P["param"], P["screen"])
     bg = spec["bg"]
     s.set_background(bg["color"], bg["light"], bg["light_color"])
-    s.build(threads, tree_on_gpu=tree_on_gpu)
+    s.build(threads, tree_on_gpu=tree_on_gpu, leaf_records=leaf_records)
     return s

@@ -62,6 +62,29 @@ def test_walk_chunks_trace_the_same_paths(require_gpu, name):
         assert rrmse(img, ref[1]) < 1e-12, (chunk, small)
 
 
+@pytest.mark.parametrize("name", ["n3_small", "n4_small", "n5_small"])
+def test_records_through_index_lists_trace_the_same_paths(require_gpu, name):
+    """Without the leaf-ordered record copy (nt_build_opts.leaf_records = -1, what a mesh gets when the
+    copy would not fit a quarter of the free memory) the walk reads a leaf's records through its index
+    list: same decisions (work counters), same image, for the direct and the staged walk variants."""
+    from math_b200 import scenes
+
+    spec = scenes.config(name)
+    a = scenes.build_scene(spec)
+    b = scenes.build_scene(spec, leaf_records=-1)
+    assert a.mesh_info(0)["device_bytes"] > b.mesh_info(0)["device_bytes"]
+    for chunk in (1, 32):
+        imgs, sts = [], []
+        for s in (a, b):
+            s.clear()
+            sts.append(s.render(spec["spp"], max_depth=spec["max_depth"], seed=8, walk_chunk=chunk))
+            imgs.append(s.image()[0])
+        for k in ("rays", "shadow_rays", "facet_tests", "box_steps", "retests", "shadow_facet_tests",
+                  "shadow_box_steps", "descent_levels"):
+            assert sts[0][k] == sts[1][k], (chunk, k)
+        assert rrmse(imgs[1], imgs[0]) < 1e-12, chunk
+
+
 def test_walk_chunk_is_validated(require_gpu):
     from math_b200 import ntrace
 
