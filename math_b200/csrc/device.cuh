@@ -358,9 +358,11 @@ __device__ __noinline__ Leaf<N> find_leaf_dfs(const MeshDev<N>& M, const Point<N
 
 // Threads per block of every kernel that walks a tree: the path caches' per-level slots are laid
 // out in shared memory with this stride.  A build-time option (NT_BLOCK, with NT_WALK_MIN_BLOCKS the
-// occupancy asked of the walk kernels).
+// occupancy asked of the walk kernels); 128 threads and 5 blocks per SM measured 8 % faster on the
+// n = 4 frame than 256 threads and 2 blocks (20 warps per SM instead of 16, at 96 registers instead
+// of 120), and 256 x 4 was slower.
 #ifndef NT_BLOCK
-#define NT_BLOCK 256
+#define NT_BLOCK 128
 #endif
 constexpr int WALK_BLOCK = NT_BLOCK;
 
@@ -396,47 +398,12 @@ __device__ __forceinline__ unsigned char* path_cache_child()
         return s_child + threadIdx.x;
 }
 
-// Resumable descents.  The descent's choice at a level depends only on the point and the box origin
-// there, so a point that makes, at every level above L, the choice the cached path made there, without
-// a tie, meets the cached path's node and origin at level L and may start there.  Per axis those
-// choices hold exactly when lo < p < hi, where lo is the origin at level L along the axis if the path
-// took the upper half there at some level above L (the origin only grows, and it is set to the mid
-// point each time; otherwise no bound beyond the root box's), and hi the least of the mid points where
-// it took the lower half (p < mid: no tie) and of the just-above-upper-bounds where it took the upper
-// one (p <= mid + h).  Each internal level a descent passes leaves its origin, bound hi and upper-half
-// mask (the state before its own choice) in one of two slots per thread (slot = level mod 2, tagged
-// with the level), so the parent and grandparent of the cached leaf can be tried first; a slot whose tag
-// matches was written on the cached path (a descent rewrites every level it passes, and the levels
-// above its start are those it shares with the path before).  Above n = 4 only the parent's slot is
-// kept (slot 0).
-template <int N>
-struct DescentSlots
-{
-        // slots per thread: parent and grandparent up to n = 4, the parent alone above (the walk
-        // kernels' static shared memory stays within 48 KB)
-        static constexpr int K = N <= 4 ? 2 : 1;
-        float* o;    // [K][N][WALK_BLOCK]
-        float* hi;   // [K][N][WALK_BLOCK]
-        int* tag;    // [K][WALK_BLOCK]: level | upper-half mask << 8
-};
-
-template <int N>
-__device__ __forceinline__ DescentSlots<N> descent_slots()
-{
-        constexpr int K = DescentSlots<N>::K;
-        __shared__ float s_o[K * N * WALK_BLOCK];
-        __shared__ float s_hi[K * N * WALK_BLOCK];
-        __shared__ int s_tag[K * WALK_BLOCK];
-        return DescentSlots<N>{s_o + threadIdx.x, s_hi + threadIdx.x, s_tag + threadIdx.x};
-}
-
 template <int N>
 __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const float* p, PathCache& pc, Leaf<N>* out,
                                                  int2* leaf_rec, unsigned* descent)
 {
         int* const fc = path_cache_slots();
         unsigned char* const cc = path_cache_child();
-        const DescentSlots<N> ds = descent_slots<N>();
 #pragma unroll
         for (int i = 0; i < N; ++i)
         {
@@ -445,60 +412,16 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                         return false;
                 }
         }
-        float o[N], hi[N];
+        float o[N];
 #pragma unroll
         for (int i = 0; i < N; ++i)
         {
                 o[i] = M.root_org[i];
-                hi[i] = INFINITY;
         }
         int node = 0;
-        int upper = 0;  // axes along which the path took the upper half at some level above
-        int start = 0;
-        // the cached leaf's parent, then its grandparent
-        constexpr int K = DescentSlots<N>::K;
-        for (int back = 1; back <= K; ++back)
-        {
-                const int L = pc.depth - back;
-                if (L < 1)
-                {
-                        break;
-                }
-                const int slot = L % K;
-                const int tag = ds.tag[slot * WALK_BLOCK];
-                if ((tag & 255) != L)
-                {
-                        continue;
-                }
-                const int up = tag >> 8;
-                bool in = true;
-#pragma unroll
-                for (int i = 0; i < N; ++i)
-                {
-                        const float so = ds.o[(slot * N + i) * WALK_BLOCK];
-                        const float sh = ds.hi[(slot * N + i) * WALK_BLOCK];
-                        in = in && p[i] < sh && (((up >> i) & 1) == 0 || p[i] > so);
-                }
-                if (in)
-                {
-#pragma unroll
-                        for (int i = 0; i < N; ++i)
-                        {
-                                o[i] = ds.o[(slot * N + i) * WALK_BLOCK];
-                                hi[i] = ds.hi[(slot * N + i) * WALK_BLOCK];
-                        }
-                        upper = up;
-                        node = fc[(L - 1) * WALK_BLOCK] + (int)cc[(L - 1) * WALK_BLOCK];
-                        start = L;
-                        break;
-                }
-        }
-        // the levels above the start count as levels of the descent (the work counters describe the
-        // full descent from the root)
-        *descent += (unsigned)start;
         bool ambiguous = false;
         bool same = pc.depth >= 0;
-        for (int lvl = start; lvl < MAX_LEVELS; ++lvl)
+        for (int lvl = 0; lvl < MAX_LEVELS; ++lvl)
         {
                 int2 nd;
                 if (same)
@@ -528,16 +451,6 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                 {
                         fc[lvl * WALK_BLOCK] = nd.x;
                 }
-                {
-                        const int slot = lvl % K;
-                        ds.tag[slot * WALK_BLOCK] = lvl | (upper << 8);
-#pragma unroll
-                        for (int i = 0; i < N; ++i)
-                        {
-                                ds.o[(slot * N + i) * WALK_BLOCK] = o[i];
-                                ds.hi[(slot * N + i) * WALK_BLOCK] = hi[i];
-                        }
-                }
                 int child = 0;
                 bool fail = false;
 #pragma unroll
@@ -545,26 +458,22 @@ __device__ __forceinline__ bool find_leaf_cached(const MeshDev<N>& M, const floa
                 {
                         float h = M.size[lvl + 1][i];
                         float mid = o[i] + h;
-                        float top = mid + h;
                         bool lo_ok = p[i] <= mid;
-                        bool hi_ok = (-p[i] <= -mid) && (p[i] <= top);
+                        bool hi_ok = (-p[i] <= -mid) && (p[i] <= mid + h);
                         if (lo_ok)
                         {
                                 ambiguous |= hi_ok;
-                                hi[i] = fminf(hi[i], mid);
                         }
                         else if (hi_ok)
                         {
                                 child |= 1 << i;
                                 o[i] = mid;
-                                hi[i] = fminf(hi[i], nextafterf(top, INFINITY));
                         }
                         else
                         {
                                 fail = true;
                         }
                 }
-                upper |= child;
                 if (fail)
                 {
                         pc.depth = -1;

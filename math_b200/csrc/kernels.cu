@@ -11,12 +11,19 @@ namespace ntrace
 namespace
 {
 constexpr int BLOCK = WALK_BLOCK;  // every wavefront kernel's block size
-// resident blocks per SM asked of the tree-walk kernels (caps their registers at 65536 / (2 x 256):
+// resident blocks per SM asked of the tree-walk kernels, which caps their registers at 65536 / (5 x
+// 128): a few spilled registers at n >= 4 cost less than the extra warps gain (with 256-thread blocks,
 // 2 blocks without spills measured faster than 3 or 4 with them)
 #ifndef NT_WALK_MIN_BLOCKS
-#define NT_WALK_MIN_BLOCKS 2
+#define NT_WALK_MIN_BLOCKS 5
 #endif
 constexpr int WALK_MIN_BLOCKS = NT_WALK_MIN_BLOCKS;
+// at n = 6 the walk state is larger: one block fewer, so that 128 registers fit without spills
+template <int N>
+constexpr int walk_min_blocks()
+{
+        return (N >= 6 && WALK_MIN_BLOCKS > 1) ? WALK_MIN_BLOCKS - 1 : WALK_MIN_BLOCKS;
+}
 // fill rounds per iteration of the lane-refill walks (1 measured faster than 2, 4, 8 or 16: a lane
 // whose new ray needs no walk waits for the next iteration rather than holding up the warp)
 #ifndef NT_FILL_ROUNDS
@@ -281,7 +288,7 @@ __device__ __forceinline__ long long warp_take(unsigned long long* work)
 
 // extension: closest object per path (ray_intersection over objects, ray_intersection.h:26-105)
 template <int N>
-__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H,
+__global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>()) k_extend(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H,
                                                   unsigned long long* counters)
 {
         const long long count = (long long)counters[C_Q_ACTIVE];
@@ -586,7 +593,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
 
 // shadow rays: light_source_is_visible (painter.cpp:172-186); visible -> add the light's share
 template <int N>
-__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum,
+__global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>()) k_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum,
                                                   unsigned long long* counters)
 {
         const long long count = (long long)counters[C_SHADOW];
@@ -846,7 +853,7 @@ __global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const D
 // closest_plan beside it), one leaf per iteration.
 // R: rounds of 32 pooled facet tests staged per warp chunk (Stage<N, R>).
 template <int N, int R>
-__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
+__global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>())
         k_extend_refill(__grid_constant__ const DevScene<N> S, PathView<N> A, HitView<N> H, const int* __restrict__ list,
                         const ClosestPlan* __restrict__ plans, unsigned long long* counters)
 {
@@ -922,7 +929,7 @@ __global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
 // Shadow rays of a scene with one mesh that walk the tree (the plan kernel's list, with the distance
 // at which each ray enters the mesh's root box): the walk runs up to the light's distance.
 template <int N, int R>
-__global__ void __launch_bounds__(BLOCK, WALK_MIN_BLOCKS)
+__global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>())
         k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, const int* __restrict__ list,
                         const float* __restrict__ entry, unsigned long long* counters)
 {
