@@ -1216,9 +1216,14 @@ double backward(nt_denoiser* d, const float* target)
         ck(gemm(LoadRows{d->dH2.as<__nv_bfloat16>(), HID}, LoadCols{d->W2.as<__nv_bfloat16>(), HID},
                 EpiMaskBF16{d->H1.as<__nv_bfloat16>(), d->dH1.as<__nv_bfloat16>(), HID}, P32, HID, HID, 0, err, s),
            "gemm dH1");
-        // weight gradients: reductions over pixels, split across CTAs
+        // weight gradients: reductions over pixels, split across CTAs, about four per SM (the products
+        // are skinny and HBM-bound, so their copies need the CTAs in flight)
         ck(cudaMemsetAsync(d->gblock.p, 0, d->gbytes(), s), "memset");
-        const int kpc = 4096;
+        int dev = 0, sms = 148;
+        ck(cudaGetDevice(&dev), "device");
+        ck(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device attribute");
+        const long long ctas = 4LL * std::max(1, sms);
+        const int kpc = (int)std::max<long long>(GK, ((long long)P32 + ctas - 1) / ctas);
         ck(gemm(LoadCols{d->dZ.as<__nv_bfloat16>(), d->Op}, LoadCols{d->H2.as<__nv_bfloat16>(), HID},
                 EpiAtomicF32{d->gW3, HID, HID}, d->Op, HID, P32, kpc, err, s),
            "gemm dW3");
