@@ -194,10 +194,10 @@ enum Counter : int
         C_Q_BASE = 19,     // queue slot of the first fresh path
         C_DONE = 20,       // 1 once every path of the pass has finished
         C_ITERS = 21,      // iterations that had work
-        // one-mesh scenes: rays that need the tree walk, compacted by the plan kernels
+        // one-mesh scenes: extension rays that need the tree walk, compacted by k_plan_extend (the
+        // shadow rays that need it are the shadow queue itself, C_SHADOW)
         C_WALK_EXT = 22,
-        C_WALK_SH = 23,
-        C_COUNT = 24
+        C_COUNT = 23
 };
 
 enum ErrorBits : int

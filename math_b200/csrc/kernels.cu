@@ -191,7 +191,8 @@ struct HitView
 template <int N>
 struct ShadowView
 {
-        float* f;        // (2N + 4) x Q: org[N], dir[N], tmax, contrib[3]
+        float* f;        // (2N + 5) x Q: org[N], dir[N], tmax, contrib[3], entry (scenes with one mesh: the
+                         // distance at which the ray enters the mesh's root box)
         uint32_t* pix;
         long long Q;
 
@@ -343,6 +344,8 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
         const long long count = (long long)counters[C_Q_ACTIVE];
         __shared__ int s_warp[BLOCK / 32];
         __shared__ long long s_base;
+        const bool one_mesh = S.nmesh == 1;
+        long long shadow_rays = 0;  // shadow rays planned here (scenes with one mesh)
         const long long tiles = (count + blockDim.x - 1) / blockDim.x;
         for (long long tile = blockIdx.x; tile < tiles; tile += gridDim.x)
         {
@@ -501,6 +504,48 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                         }
                                 }
                         }
+                        // scenes with one mesh: the shadow ray's object plan here, on the ray in registers (as
+                        // closest_plan does for extension rays): a non-mesh object nearer than the light
+                        // occludes it; a ray whose mesh root box starts beyond the light (or is missed) reaches
+                        // the light and adds its share now; only the rays that must walk the mesh are queued,
+                        // with the distance at which they enter its root box
+                        float sh_entry = 0;
+                        if (one_mesh && shadow)
+                        {
+                                ++shadow_rays;
+                                Ray<N> r;
+#pragma unroll
+                                for (int k = 0; k < N; ++k)
+                                {
+                                        r.org[k] = sh_org[k];
+                                        r.dir[k] = sh_dir[k];
+                                }
+                                bool occluded = false;
+                                bool walk = false;
+                                for (int o = 0; o < S.nobj; ++o)
+                                {
+                                        float a;
+                                        if (!obj_approx<N>(S, o, r, &a) || !(a < sh_tmax))
+                                        {
+                                                continue;
+                                        }
+                                        if (S.obj[o].kind == OBJ_MESH)
+                                        {
+                                                walk = true;
+                                                sh_entry = a;
+                                        }
+                                        else
+                                        {
+                                                occluded = true;
+                                        }
+                                }
+                                walk = walk && !occluded;
+                                if (!occluded && !walk)
+                                {
+                                        accumulate(accum, pixel, sh_c[0], sh_c[1], sh_c[2]);
+                                }
+                                shadow = walk;
+                        }
                         long long qo = compact_slot(shadow, counters + C_SHADOW, s_warp, &s_base);
                         if (shadow)
                         {
@@ -514,6 +559,7 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                                 SQ.at(2 * N + 1, qo) = sh_c[0];
                                 SQ.at(2 * N + 2, qo) = sh_c[1];
                                 SQ.at(2 * N + 3, qo) = sh_c[2];
+                                SQ.at(2 * N + 4, qo) = sh_entry;
                                 SQ.pix[qo] = pixel;
                         }
                         if (S.smooth_normal)
@@ -588,6 +634,10 @@ __global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScen
                 {
                         atomicOr((unsigned long long*)(counters + C_ERROR), (unsigned long long)err);
                 }
+        }
+        if (one_mesh)
+        {
+                warp_add(counters + C_SHADOW_RAYS, shadow_rays);
         }
 }
 
@@ -787,68 +837,6 @@ __global__ void __launch_bounds__(BLOCK) k_plan_extend(__grid_constant__ const D
         warp_add(counters + C_RAYS, rays);
 }
 
-// Shadow rays of a scene with one mesh, first pass: a non-mesh object nearer than the light occludes
-// at once; a ray whose mesh root box starts beyond the light (or is missed) reaches the light and adds
-// its contribution here; the rest are compacted into the walk list for k_shadow_refill.
-template <int N>
-__global__ void __launch_bounds__(BLOCK) k_plan_shadow(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ,
-                                                       double* accum, int* __restrict__ list, float* __restrict__ entry,
-                                                       unsigned long long* counters)
-{
-        const long long count = (long long)counters[C_SHADOW];
-        const int lane = threadIdx.x & 31;
-        const long long warps = (long long)gridDim.x * (blockDim.x >> 5);
-        long long rays = 0;
-        for (long long w0 = ((long long)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5)) * 32; w0 < count;
-             w0 += warps * 32)
-        {
-                const long long j = w0 + lane;
-                bool walk = false;
-                float a_m = 0;
-                if (j < count)
-                {
-                        ++rays;
-                        Ray<N> r;
-#pragma unroll
-                        for (int k = 0; k < N; ++k)
-                        {
-                                r.org[k] = SQ.at(k, j);
-                                r.dir[k] = SQ.at(N + k, j);
-                        }
-                        const float dj = SQ.at(2 * N, j);
-                        bool occluded = false;
-                        for (int o = 0; o < S.nobj; ++o)
-                        {
-                                float a;
-                                if (!obj_approx<N>(S, o, r, &a) || !(a < dj))
-                                {
-                                        continue;
-                                }
-                                if (S.obj[o].kind == OBJ_MESH)
-                                {
-                                        walk = true;
-                                        a_m = a;
-                                }
-                                else
-                                {
-                                        occluded = true;
-                                }
-                        }
-                        walk = walk && !occluded;
-                        if (!occluded && !walk)
-                        {
-                                accumulate(accum, SQ.pix[j], SQ.at(2 * N + 1, j), SQ.at(2 * N + 2, j), SQ.at(2 * N + 3, j));
-                        }
-                }
-                const long long q = list_append(walk, j, list, counters + C_WALK_SH);
-                if (q >= 0)
-                {
-                        entry[q] = a_m;
-                }
-        }
-        warp_add(counters + C_SHADOW_RAYS, rays);
-}
-
 // Extension rays of a scene with one mesh that walk the tree (the plan kernel's list, with each ray's
 // closest_plan beside it), one leaf per iteration.
 // R: rounds of 32 pooled facet tests staged per warp chunk (Stage<N, R>).
@@ -926,14 +914,13 @@ __global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>())
         flush_stats<false>(counters, ws, rays, 0);
 }
 
-// Shadow rays of a scene with one mesh that walk the tree (the plan kernel's list, with the distance
+// Shadow rays of a scene with one mesh that walk the tree (k_shade queued only those, with the distance
 // at which each ray enters the mesh's root box): the walk runs up to the light's distance.
 template <int N, int R>
 __global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>())
-        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, const int* __restrict__ list,
-                        const float* __restrict__ entry, unsigned long long* counters)
+        k_shadow_refill(__grid_constant__ const DevScene<N> S, ShadowView<N> SQ, double* accum, unsigned long long* counters)
 {
-        const long long count = (long long)counters[C_WALK_SH];
+        const long long count = (long long)counters[C_SHADOW];
         const MeshDev<N>& M = S.mesh[0];
         WalkStats ws{0, 0, 0, 0, 0};
         long long rays = 0;
@@ -949,7 +936,7 @@ __global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>())
                         const long long q = lane_refill(i < 0, counters + C_WORK_SH, count, &exhausted);
                         if (q >= 0)
                         {
-                                const long long j = list[q];
+                                const long long j = q;
                                 Ray<N> r;
 #pragma unroll
                                 for (int k = 0; k < N; ++k)
@@ -957,10 +944,10 @@ __global__ void __launch_bounds__(BLOCK, walk_min_blocks<N>())
                                         r.org[k] = SQ.at(k, j);
                                         r.dir[k] = SQ.at(N + k, j);
                                 }
-                                // listed by k_plan_shadow: nothing nearer than the light occludes it, and the
-                                // mesh's root box starts before the light at entry[q]
+                                // queued by k_shade: nothing nearer than the light occludes it, and the mesh's
+                                // root box starts before the light at the stored entry distance
                                 const float dj = SQ.at(2 * N, j);
-                                walk_begin<N>(w, r, entry[q], dj);
+                                walk_begin<N>(w, r, SQ.at(2 * N + 4, j), dj);
                                 dist = dj;
                                 i = j;
                         }
@@ -1127,7 +1114,6 @@ __global__ void k_iter_begin(unsigned long long* c, long long total, long long Q
         c[C_SHADOW] = 0;
         c[C_SMOOTH] = 0;
         c[C_WALK_EXT] = 0;
-        c[C_WALK_SH] = 0;
         if (active + fresh > 0)
         {
                 c[C_ITERS] += 1;
@@ -1219,10 +1205,9 @@ size_t Wavefront<N>::bytes_for(long long Q, int lights, bool smooth)
         size_t per_path = sizeof(float) * (2 * N + 4) * 2  // path state A and B
                           + sizeof(uint32_t) * 2 * 2 + sizeof(int) * 2
                           + sizeof(float) + sizeof(int) * 2  // hit record
-                          + (sizeof(float) * (2 * N + 4) + sizeof(uint32_t)) * (size_t)lights * (smooth ? 2 : 1)  // shadow queues
-                          + sizeof(int) * (1 + (size_t)lights)  // walk lists
-                          + 32 + sizeof(float) * (size_t)lights;  // the plans of the listed rays
-        return per_path * (size_t)Q + 22 * 256;
+                          + (sizeof(float) * (2 * N + 5) + sizeof(uint32_t)) * (size_t)lights * (smooth ? 2 : 1)  // shadow queues
+                          + sizeof(int) + 32;  // the extension walk list and its rays' plans
+        return per_path * (size_t)Q + 20 * 256;
 }
 
 template <int N>
@@ -1246,15 +1231,13 @@ void Wavefront<N>::carve(char* base, long long Q, int lights, bool smooth)
         hit_t = (float*)take(sizeof(float) * Q);
         hit_obj = (int*)take(sizeof(int) * Q);
         hit_facet = (int*)take(sizeof(int) * Q);
-        sq_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
+        sq_f = (float*)take(sizeof(float) * (2 * N + 5) * Q * lights);
         sq_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
         walk_ext = (int*)take(sizeof(int) * Q);
-        walk_sh = (int*)take(sizeof(int) * Q * lights);
         plan_ext = take(32 * Q);
-        plan_sh = (float*)take(sizeof(float) * Q * lights);
         if (smooth)
         {
-                sm_f = (float*)take(sizeof(float) * (2 * N + 4) * Q * lights);
+                sm_f = (float*)take(sizeof(float) * (2 * N + 5) * Q * lights);
                 sm_pix = (uint32_t*)take(sizeof(uint32_t) * Q * lights);
         }
         else
@@ -1375,10 +1358,6 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         {
                 cudaEventRecord(ev[4], st);
         }
-        if (one_mesh)
-        {
-                k_plan_shadow<N><<<str_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
-        }
         if (ev)
         {
                 cudaEventRecord(ev[5], st);
@@ -1387,19 +1366,19 @@ void Wavefront<N>::enqueue_iteration(const DevScene<N>& S, const PassDev& P, dou
         {
                 if (vi == 0)
                 {
-                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
+                        k_shadow_refill<N, 0><<<sh_grid, BLOCK, 0, st>>>(S, SQ, accum, counters);
                 }
                 else if (vi == 1)
                 {
-                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
+                        k_shadow_refill<N, 1><<<sh_grid, BLOCK, Stage<N, 1>::BYTES, st>>>(S, SQ, accum, counters);
                 }
                 else if (vi == 2)
                 {
-                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
+                        k_shadow_refill<N, 2><<<sh_grid, BLOCK, Stage<N, 2>::BYTES, st>>>(S, SQ, accum, counters);
                 }
                 else
                 {
-                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, walk_sh, plan_sh, counters);
+                        k_shadow_refill<N, 4><<<sh_grid, BLOCK, Stage<N, 4>::BYTES, st>>>(S, SQ, accum, counters);
                 }
         }
         else

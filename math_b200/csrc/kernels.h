@@ -55,13 +55,11 @@ struct Wavefront
         int* hit_facet = nullptr;
         float* sq_f = nullptr;
         uint32_t* sq_pix = nullptr;
-        // one-mesh scenes: queue indices of the extension and shadow rays that walk the tree, and what
-        // the plan kernels found for them (the extension rays' object plan, 32 bytes each; the shadow
-        // rays' mesh entry distance), so that the walk kernels do not work it out again
+        // one-mesh scenes: queue indices of the extension rays that walk the tree, and the object plan
+        // k_plan_extend found for each (32 bytes), so that the walk kernel does not work it out again
+        // (the shadow queue holds only rays that walk, with their entry distance: k_shade plans them)
         int* walk_ext = nullptr;
-        int* walk_sh = nullptr;
         void* plan_ext = nullptr;
-        float* plan_sh = nullptr;
         // smooth-normal shadow queue (only when some mesh has vertex normals and smooth_normal is set)
         float* sm_f = nullptr;
         uint32_t* sm_pix = nullptr;
@@ -88,7 +86,7 @@ struct Wavefront
                                cudaEvent_t* ev) const;
         static int iteration_launches(bool smooth, bool one_mesh)
         {
-                return 6 + (smooth ? 1 : 0) + (one_mesh ? 2 : 0);
+                return 6 + (smooth ? 1 : 0) + (one_mesh ? 1 : 0);
         }
 
         // The iteration kernels' attributes (dynamic shared memory of the walk kernels) and grid sizes,
