@@ -18,6 +18,14 @@ constexpr int BLOCK = WALK_BLOCK;  // every wavefront kernel's block size
 #define NT_WALK_MIN_BLOCKS 5
 #endif
 constexpr int WALK_MIN_BLOCKS = NT_WALK_MIN_BLOCKS;
+// resident blocks per SM asked of the shading kernel (a build-time option): 8 blocks of 128 caps it at
+// 64 registers, 32 warps per SM instead of 16 at the 108 it takes uncapped; the kernel is bound by
+// latency at that occupancy (ncu: 47 % issue, 13 % of DRAM bandwidth), and the n = 4 frame measured
+// 40.5 -> 38.3 ms with the cap despite a few spilled registers
+#ifndef NT_SHADE_MIN_BLOCKS
+#define NT_SHADE_MIN_BLOCKS 8
+#endif
+constexpr int SHADE_MIN_BLOCKS = NT_SHADE_MIN_BLOCKS;
 // at n = 6 the walk state is larger: one block fewer, so that 128 registers fit without spills
 template <int N>
 constexpr int walk_min_blocks()
@@ -337,7 +345,7 @@ __device__ __forceinline__ void accumulate(double* accum, uint32_t pixel, float 
 // or an emitting hit adds its colour to the pixel; a diffuse hit emits one shadow ray per light into
 // the shadow queue and, below the depth cap, writes its continuation into the next path queue.
 template <int N>
-__global__ void __launch_bounds__(BLOCK) k_shade(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, HitView<N> H,
+__global__ void __launch_bounds__(BLOCK, SHADE_MIN_BLOCKS) k_shade(__grid_constant__ const DevScene<N> S, const PassDev P, PathView<N> A, HitView<N> H,
                                                  PathView<N> B, ShadowView<N> SQ, ShadowView<N> SM, double* accum,
                                                  unsigned long long* counters)
 {
