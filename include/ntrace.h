@@ -118,8 +118,9 @@ typedef struct nt_stats
         int64_t shadow_retests;
         int64_t shadow_descent_levels;
         int64_t iterations;       /* wavefront iterations that had work */
-        double plan_ms;           /* device time of the plan-and-compact kernels of one-mesh scenes (timing = 1):
-                                     they finish the rays that need no tree walk and list the others */
+        double plan_ms;           /* device time of the extension rays' plan-and-compact kernel of one-mesh
+                                     scenes (timing = 1): it finishes the rays that need no tree walk and lists
+                                     the others (the shadow rays' plan runs inside the shading kernel, shade_ms) */
 } nt_stats;
 
 typedef struct nt_mesh_info
