@@ -52,6 +52,27 @@ def _box_params(n):
     return dor.join(parts)
 
 
+def test_gemm_entry_points_validate_their_shapes_before_any_device_work():
+    """The GEMM entry points refuse shapes the kernel cannot take (N not a multiple of 16 or above 256;
+    for the transposed form M not a multiple of 8) with NT_EINVAL, before touching the device."""
+    import ctypes
+
+    from math_b200 import ntrace
+
+    lib = ntrace.library()
+    vp = ctypes.c_void_p
+    lib.nt_tc_gemm_bf16.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    lib.nt_tc_gemm_bf16_t.argtypes = [vp, vp, vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, vp]
+    buf = ctypes.create_string_buffer(64)
+    p = ctypes.cast(buf, vp)
+    assert lib.nt_tc_gemm_bf16(p, p, p, 16, 8, 16, None) == ntrace.NT_EINVAL
+    assert lib.nt_tc_gemm_bf16(p, p, p, 16, 272, 16, None) == ntrace.NT_EINVAL
+    assert lib.nt_tc_gemm_bf16(None, p, p, 16, 16, 16, None) == ntrace.NT_EINVAL
+    assert lib.nt_tc_gemm_bf16_t(p, p, p, 12, 16, 64, 0, None) == ntrace.NT_EINVAL
+    assert lib.nt_tc_gemm_bf16_t(p, p, p, 16, 24, 64, 0, None) == ntrace.NT_EINVAL
+    assert lib.nt_tc_gemm_bf16_t(p, p, p, 16, 16, 64, -1, None) == ntrace.NT_EINVAL
+
+
 def test_bf16_rounding_is_nearest_even():
     x = np.array([1.0, 1.00390625, 1.005859375, 1.0078125, -2.5, 3.0e-39, 1.0 + 2 ** -8 + 2 ** -9], np.float32)
     got = dor.bf16(x)
